@@ -1,0 +1,13 @@
+"""B200 creature-evaluation engine.
+
+Runs the evolution simulator's per-creature position-based-dynamics trials
+(the reference's shaders/creature.cu path) on sm_100a GPUs behind a C ABI
+(include/creature_engine.h). This package holds the CUDA kernels and host
+library sources (csrc/), their build (build.py), the ctypes binding of the C
+ABI (api.py) and the seeded workloads (configs.py).
+"""
+from .api import (  # noqa: F401
+    CE_ERR_BUSY, CE_ERR_DEVICE, CE_ERR_INVALID, CE_ERR_OOM, CE_ERR_TIMEOUT, CE_ERR_UNSUPPORTED, CE_OK,
+    EXPORTED, FLAG_NAMES, METRICS_DTYPE, RESULT_DTYPE, RESULT_FIELDS, Engine, EngineError, GenSpecPy, Params,
+    Population, WavePack, World, evaluate, frame_stride, generate, lib, make_params, make_world, niche, pack,
+    settle_frames, to_metrics, trial_steps, world_flags)

@@ -1,0 +1,565 @@
+"""Python host side of the creature engine: a ctypes binding of the C ABI in
+include/creature_engine.h.
+
+It mirrors the reference's engine surface for this path:
+
+* ``Engine`` is ``trait Engine`` (src/engine.rs:163-199): ``submit``,
+  ``poll``, ``wait``, ``free_slots``, ``allocated_bytes``, plus ``record``
+  (``record_on_gpu``, src/engine.rs:71-92) and ``release_idle``.
+* ``evaluate`` is ``Gpu::evaluate`` (src/gpu.rs:46-57): results in population
+  order.
+* ``pack`` is ``kernel::pack`` (src/kernel.rs:429-593) and ``make_params`` is
+  ``kernel::params`` (src/kernel.rs:212-251).
+* ``to_metrics`` and ``niche`` are ``scheduler::to_metrics``
+  (src/scheduler.rs:890-923) and ``Descriptor::niche_in`` with ``cell_index``
+  (src/qd.rs:762-846, 988-999).
+
+Every call runs the compiled library; there is no Python or CPU stand-in for
+the GPU path. A missing library or a missing GPU is an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libcreature_engine.so"
+
+# ------------------------------------------------------------------ status
+CE_OK, CE_ERR_INVALID, CE_ERR_OOM, CE_ERR_TIMEOUT, CE_ERR_DEVICE, CE_ERR_UNSUPPORTED, CE_ERR_BUSY = range(7)
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "OOM", 3: "TIMEOUT", 4: "DEVICE", 5: "UNSUPPORTED", 6: "BUSY"}
+
+MAX_NODES = 32
+MAX_MUSCLES = 96
+NODE_WORDS = 6
+BONE_WORDS = 6
+MUSCLE_FIELDS = 20
+SUBSTEPS = 16
+NO_SENSOR = 255
+
+FLAG_NAMES = ["GROUND", "TERRAIN", "SLOPE", "GAPS", "HURDLES", "QUAKE", "MUD", "WATER", "ICE", "WIND", "AIR",
+              "BRAMBLES"]
+
+
+class EngineError(RuntimeError):
+    """A failed engine call; ``status`` is the ce_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+    @property
+    def out_of_memory(self) -> bool:
+        return self.status == CE_ERR_OOM
+
+
+# ------------------------------------------------------------- structures
+class Rung(C.Structure):
+    _fields_ = [("w", C.c_float * 6), ("bias", C.c_float), ("off", C.c_uint32)]
+
+
+class World(C.Structure):
+    _fields_ = [
+        ("ground", C.c_uint32), ("terrain", C.c_uint32),
+        ("gravity", C.c_float), ("air_retention", C.c_float), ("ground_friction", C.c_float),
+        ("muscle_energy", C.c_float), ("muscle_recovery", C.c_float),
+        ("slope", C.c_float), ("wind", C.c_float), ("mud", C.c_float), ("brambles", C.c_float),
+        ("water", C.c_float), ("patches", C.c_float), ("gaps", C.c_float), ("hurdles", C.c_float),
+        ("quake", C.c_float), ("duration", C.c_float), ("rate", C.c_uint32),
+        ("has_screen", C.c_uint32), ("screen_seconds", C.c_float), ("screen_bar", C.c_float),
+        ("screen_bar_young", C.c_float), ("screen_bar_reshaped", C.c_float),
+        ("has_rungs", C.c_uint32), ("rungs", Rung * 2),
+    ]
+
+
+PARAM_FIELDS = ["count", "base", "steps", "screen_step", "stride", "gravity", "air", "friction", "terrain",
+                "muscle_energy", "muscle_recovery", "slope", "wind", "mud", "gaps", "hurdles", "quake",
+                "screen_bar", "screen_bar_young", "screen_bar_reshaped", "water", "patches", "air_sub",
+                "inv_muscle_energy", "brambles"]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_uint32 if i < 5 else C.c_float) for i, n in enumerate(PARAM_FIELDS)] + [
+        ("r1", Rung), ("r2", Rung)]
+
+
+RESULT_FIELDS = ["fitness", "ground_contact", "vertical_oscillation", "gait_frequency", "previous_center_y",
+                 "vertical_extremum", "vertical_trend", "gait_turns", "height_sum", "contact_lo", "contact_hi",
+                 "lift_lo", "lift_hi", "ground_lo", "ground_hi", "fall_time", "head_shake", "screen_x",
+                 "screened"]
+RESULT_DTYPE = np.dtype([(n, "<f4") for n in RESULT_FIELDS])
+NODE_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("diameter", "<f4"), ("friction", "<f4")])
+BONE_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("rest_length", "<f4"), ("min_angle", "<f4"),
+                       ("max_angle", "<f4"), ("organ_mass", "<f4"), ("organ_at", "<f4")])
+MUSCLE_DTYPE = np.dtype([("bone_a", "<u4"), ("bone_b", "<u4"), ("anchor_a", "<f4"), ("anchor_b", "<f4"),
+                         ("short", "<f4"), ("long", "<f4"), ("period", "<f4"), ("phase", "<f4"),
+                         ("duty", "<f4"), ("stiffness", "<f4"), ("sensor", "<u4"), ("reset", "<f4"),
+                         ("tendon", "<f4")])
+GENOME_DTYPE = np.dtype([("node_start", "<u4"), ("node_count", "<u4"), ("bone_start", "<u4"),
+                         ("bone_count", "<u4"), ("muscle_start", "<u4"), ("muscle_count", "<u4"),
+                         ("id", "<u8"), ("flags", "<u4"), ("reserved", "<u4")])
+METRICS_DTYPE = np.dtype([("fitness", "<f4"), ("ground_contact", "<f4"), ("vertical_oscillation", "<f4"),
+                          ("gait_frequency", "<f4"), ("mean_height", "<f4"), ("feet", "<f4"),
+                          ("screen_x", "<f4"), ("screened", "<u4"), ("steps", "<u4")])
+
+
+class PopulationC(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("bones", C.c_void_p), ("muscles", C.c_void_p), ("genomes", C.c_void_p),
+                ("count", C.c_size_t), ("strength_scale", C.c_void_p)]
+
+
+class WavePackC(C.Structure):
+    _fields_ = [("lanes", C.c_void_p), ("lanes_len", C.c_size_t), ("muscles", C.c_void_p),
+                ("muscles_len", C.c_size_t), ("heads", C.c_void_p), ("count", C.c_size_t)]
+
+
+class GenSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("min_nodes", C.c_uint32), ("max_nodes", C.c_uint32),
+                ("node_dist", C.c_uint32), ("mean_nodes", C.c_float), ("min_muscles", C.c_uint32),
+                ("max_muscles", C.c_uint32), ("muscle_rule", C.c_uint32), ("max_extra", C.c_uint32),
+                ("joint_lo_deg", C.c_float), ("joint_hi_deg", C.c_float), ("friction_lo", C.c_float),
+                ("friction_hi", C.c_float), ("first_id", C.c_uint64)]
+
+
+class Options(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("warps_per_cta", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
+
+
+# --------------------------------------------------------------- library
+_LIB: Optional[C.CDLL] = None
+
+
+def _bind(lib: C.CDLL) -> None:
+    P = C.POINTER
+    sigs = {
+        "ce_world_flags": (C.c_uint32, [P(World)]),
+        "ce_make_params": (C.c_int, [P(World), C.c_uint32, C.c_uint32, C.c_uint32, P(Params)]),
+        "ce_pack_size": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(C.c_size_t), P(C.c_size_t)]),
+        "ce_pack": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_frame_stride": (C.c_uint32, [C.c_uint32]),
+        "ce_generate_size": (C.c_int, [P(GenSpec), C.c_size_t, P(C.c_size_t), P(C.c_size_t), P(C.c_size_t)]),
+        "ce_generate": (C.c_int, [P(GenSpec), C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+        "ce_to_metrics": (C.c_int, [C.c_void_p, C.c_uint32, P(World), C.c_void_p]),
+        "ce_niche": (C.c_int64, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_int, C.c_void_p]),
+        "ce_open": (C.c_int, [C.c_int, P(Options), P(C.c_void_p)]),
+        "ce_close": (C.c_int, [C.c_void_p]),
+        "ce_last_error": (C.c_char_p, []),
+        "ce_submit": (C.c_int, [C.c_void_p, P(WavePackC), P(World), P(C.c_uint64)]),
+        "ce_poll": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_uint64), C.c_void_p, C.c_size_t, P(C.c_size_t),
+                              P(C.c_double)]),
+        "ce_wait": (C.c_int, [C.c_void_p, C.c_int64]),
+        "ce_free_slots": (C.c_int, [C.c_void_p]),
+        "ce_allocated_bytes": (C.c_size_t, [C.c_void_p]),
+        "ce_release_idle": (C.c_int, [C.c_void_p]),
+        "ce_record": (C.c_int, [C.c_void_p, P(WavePackC), P(World), C.c_void_p, C.c_size_t, C.c_void_p]),
+        "ce_advance_scratch_bytes": (C.c_size_t, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+        "ce_advance_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, P(Params), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_void_p]),
+        "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def lib() -> C.CDLL:
+    """The engine library, loaded once. Raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m evolution_simulator_gpu_b200.build")
+        _LIB = C.CDLL(str(LIB_PATH))
+        _bind(_LIB)
+    return _LIB
+
+
+EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_frame_stride", "ce_generate_size",
+            "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
+            "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
+            "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault"]
+
+
+def _check(status: int, what: str) -> None:
+    if status != CE_OK:
+        msg = lib().ce_last_error().decode(errors="replace")
+        raise EngineError(status, f"{what}: {msg}")
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+# ------------------------------------------------------------------ worlds
+def make_world(**kw) -> World:
+    """A world with the reference's default settings (src/config.rs:119-161):
+    flat calm ground, 9.8 m/s^2, grip 1.5, 20 s trials at 60 steps a second,
+    no screen and no rungs. Keyword arguments override fields."""
+    w = World()
+    w.ground = 1
+    w.terrain = 0
+    w.gravity = 9.8
+    w.air_retention = 1.0
+    w.ground_friction = 1.5
+    w.muscle_energy = 1.0
+    w.muscle_recovery = 1.0
+    w.duration = 20.0
+    w.rate = 60
+    for k, v in kw.items():
+        if k == "rungs":
+            w.has_rungs = 1
+            for i, r in enumerate(v):
+                w.rungs[i].w[:] = list(r[0])
+                w.rungs[i].bias = r[1]
+                w.rungs[i].off = r[2]
+        elif k == "screen":
+            seconds, bar = v[0], v[1]
+            young = v[2] if len(v) > 2 else bar
+            reshaped = v[3] if len(v) > 3 else bar
+            w.has_screen = 1
+            w.screen_seconds, w.screen_bar, w.screen_bar_young, w.screen_bar_reshaped = seconds, bar, young, reshaped
+        else:
+            setattr(w, k, v)
+    return w
+
+
+def world_flags(w: World) -> int:
+    return int(lib().ce_world_flags(C.byref(w)))
+
+
+def make_params(w: World, base: int = 0, count: int = 0, stride: int = 0) -> Params:
+    p = Params()
+    _check(lib().ce_make_params(C.byref(w), base, count, stride, C.byref(p)), "ce_make_params")
+    return p
+
+
+def settle_frames(w: World) -> int:
+    rate = w.rate or 60
+    return (200 * rate + 119) // 120
+
+
+def trial_steps(w: World) -> int:
+    return int(np.round(np.float32(w.duration) * np.float32(w.rate or 60)))
+
+
+# -------------------------------------------------------------- population
+@dataclasses.dataclass
+class Population:
+    """An arena-packed population (src/evolution.rs:440-453)."""
+    nodes: np.ndarray
+    bones: np.ndarray
+    muscles: np.ndarray
+    genomes: np.ndarray
+    strength: Optional[np.ndarray] = None
+
+    def __len__(self) -> int:
+        return len(self.genomes)
+
+    def c(self) -> PopulationC:
+        return PopulationC(_ptr(self.nodes), _ptr(self.bones), _ptr(self.muscles), _ptr(self.genomes),
+                           len(self.genomes), _ptr(self.strength))
+
+    def creature(self, i: int):
+        g = self.genomes[i]
+        n = self.nodes[g["node_start"]:g["node_start"] + g["node_count"]]
+        b = self.bones[g["bone_start"]:g["bone_start"] + g["bone_count"]]
+        m = self.muscles[g["muscle_start"]:g["muscle_start"] + g["muscle_count"]]
+        s = None if self.strength is None else self.strength[g["muscle_start"]:g["muscle_start"] + g["muscle_count"]]
+        return n, b, m, s
+
+    def subset(self, idx) -> "Population":
+        """The creatures at `idx`, in that order, as a population of their own."""
+        parts = [self.creature(int(i)) for i in idx]
+        nodes = np.concatenate([p[0] for p in parts]) if parts else np.zeros(0, NODE_DTYPE)
+        bones = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, BONE_DTYPE)
+        muscles = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, MUSCLE_DTYPE)
+        strength = None
+        if self.strength is not None:
+            strength = np.concatenate([p[3] for p in parts]).astype(np.float32) if parts else np.zeros(0, np.float32)
+        genomes = np.zeros(len(parts), GENOME_DTYPE)
+        an = ab = am = 0
+        for k, (i, p) in enumerate(zip(idx, parts)):
+            g = self.genomes[int(i)]
+            genomes[k] = (an, len(p[0]), ab, len(p[1]), am, len(p[2]), g["id"], g["flags"], 0)
+            an += len(p[0])
+            ab += len(p[1])
+            am += len(p[2])
+        return Population(nodes, bones, muscles, genomes, strength)
+
+
+@dataclasses.dataclass
+class GenSpecPy:
+    seed: int
+    min_nodes: int = 3
+    max_nodes: int = 6
+    node_dist: int = 0  # 0 uniform, 1 geometric
+    mean_nodes: float = 7.0
+    min_muscles: int = 2
+    max_muscles: int = 24
+    muscle_rule: int = 0  # 0 spanning + extras, 1 count uniform in [min, max]
+    max_extra: int = 3
+    joint_lo_deg: float = 120.0
+    joint_hi_deg: float = 120.0
+    friction_lo: float = 0.0
+    friction_hi: float = 1.0
+    first_id: int = 1
+
+    def c(self) -> GenSpec:
+        return GenSpec(self.seed, self.min_nodes, self.max_nodes, self.node_dist, self.mean_nodes,
+                       self.min_muscles, self.max_muscles, self.muscle_rule, self.max_extra, self.joint_lo_deg,
+                       self.joint_hi_deg, self.friction_lo, self.friction_hi, self.first_id)
+
+
+def generate(spec: GenSpecPy, count: int, first: int = 0) -> Population:
+    """`count` seeded synthetic creatures; creature i is a function of
+    (spec.seed, first + i) only."""
+    L = lib()
+    cs = spec.c()
+    nn, nb, nm = C.c_size_t(), C.c_size_t(), C.c_size_t()
+    if first == 0:
+        _check(L.ce_generate_size(C.byref(cs), count, C.byref(nn), C.byref(nb), C.byref(nm)), "ce_generate_size")
+        sizes = (nn.value, nb.value, nm.value)
+    else:
+        sizes = (count * MAX_NODES, count * MAX_NODES, count * MAX_MUSCLES)
+    nodes = np.zeros(sizes[0], NODE_DTYPE)
+    bones = np.zeros(sizes[1], BONE_DTYPE)
+    muscles = np.zeros(sizes[2], MUSCLE_DTYPE)
+    strength = np.zeros(sizes[2], np.float32)
+    genomes = np.zeros(count, GENOME_DTYPE)
+    _check(L.ce_generate(C.byref(cs), first, count, _ptr(nodes), _ptr(bones), _ptr(muscles), _ptr(strength),
+                         _ptr(genomes)), "ce_generate")
+    if first != 0 and count:
+        last = genomes[-1]
+        nodes = nodes[:last["node_start"] + last["node_count"]].copy()
+        bones = bones[:last["bone_start"] + last["bone_count"]].copy()
+        muscles = muscles[:last["muscle_start"] + last["muscle_count"]].copy()
+        strength = strength[:last["muscle_start"] + last["muscle_count"]].copy()
+    return Population(nodes, bones, muscles, genomes, strength)
+
+
+# --------------------------------------------------------------- packing
+@dataclasses.dataclass
+class WavePack:
+    """Packed records of a batch (src/kernel.rs:56-72), sorted by (muscles,
+    nodes, population index). `slots[c]` is the position in the packed
+    indices of packed creature c; `info` holds node, bone and muscle counts
+    and the quake hash."""
+    lanes: np.ndarray
+    muscles: np.ndarray
+    heads: np.ndarray
+    slots: np.ndarray
+    info: np.ndarray
+
+    def __len__(self) -> int:
+        return len(self.slots)
+
+    def c(self) -> WavePackC:
+        return WavePackC(_ptr(self.lanes), len(self.lanes), _ptr(self.muscles), len(self.muscles),
+                         _ptr(self.heads), len(self.slots))
+
+    def take(self, packed_positions) -> "WavePack":
+        """A batch of its own with the packed creatures at `packed_positions`
+        (their record offsets rewritten), in that order."""
+        pos = np.asarray(packed_positions, dtype=np.int64)
+        lanes, muscles, heads = [], [], np.zeros((len(pos), 8), np.uint32)
+        rl = ml = 0
+        for k, c in enumerate(pos):
+            h = self.heads[c].copy()
+            n, m = int(h[0] & 255), int(h[1])
+            r0, m0 = int(h[3]), int(h[4])
+            rlen = n * NODE_WORDS + (n - 1) * BONE_WORDS
+            lanes.append(self.lanes[r0:r0 + rlen])
+            muscles.append(self.muscles[m0:m0 + m * MUSCLE_FIELDS])
+            h[3], h[4] = rl, ml
+            heads[k] = h
+            rl += rlen
+            ml += m * MUSCLE_FIELDS
+        lanes_a = np.concatenate(lanes) if lanes else np.zeros(1, np.uint32)
+        mus_a = np.concatenate(muscles) if muscles and ml else np.zeros(1, np.float32)
+        return WavePack(np.ascontiguousarray(lanes_a, np.uint32), np.ascontiguousarray(mus_a, np.float32),
+                        heads, self.slots[pos].copy(), self.info[pos].copy())
+
+    @property
+    def max_muscles(self) -> int:
+        return int(self.heads[:, 1].max()) if len(self) else 0
+
+    @property
+    def max_nodes(self) -> int:
+        return int((self.heads[:, 0] & 255).max()) if len(self) else 0
+
+
+def pack(pop: Population, world: World, indices=None) -> WavePack:
+    L = lib()
+    pc = pop.c()
+    idx = None if indices is None else np.ascontiguousarray(indices, np.uint32)
+    n = len(pop) if idx is None else len(idx)
+    rl, ml = C.c_size_t(), C.c_size_t()
+    _check(L.ce_pack_size(C.byref(pc), _ptr(idx), n, C.byref(rl), C.byref(ml)), "ce_pack_size")
+    lanes = np.zeros(rl.value, np.uint32)
+    muscles = np.zeros(ml.value, np.float32)
+    heads = np.zeros((n, 8), np.uint32)
+    slots = np.zeros(n, np.uint32)
+    info = np.zeros((n, 4), np.uint32)
+    _check(L.ce_pack(C.byref(pc), _ptr(idx), n, C.byref(world), _ptr(lanes), _ptr(muscles), _ptr(heads),
+                     _ptr(slots), _ptr(info)), "ce_pack")
+    return WavePack(lanes, muscles, heads, slots, info)
+
+
+def frame_stride(max_muscles: int) -> int:
+    return int(lib().ce_frame_stride(max_muscles))
+
+
+# ----------------------------------------------------------------- engine
+class Engine:
+    """One GPU's engine (the reference's ThreadedEngine surface)."""
+
+    def __init__(self, device: int = 0, slots: int = 0, ctas_per_sm: int = 0):
+        h = C.c_void_p()
+        opts = Options(slots, ctas_per_sm, 0)
+        _check(lib().ce_open(device, C.byref(opts), C.byref(h)), "ce_open")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise EngineError(CE_ERR_INVALID, "engine is closed")
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().ce_close(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self) -> "Engine":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def name(self) -> str:
+        return f"b200-cuda:{self.device}"
+
+    def max_nodes(self) -> int:
+        return MAX_NODES
+
+    def submit(self, wave: WavePack, world: World) -> int:
+        t = C.c_uint64()
+        _check(lib().ce_submit(self.handle, C.byref(wave.c()), C.byref(world), C.byref(t)), "ce_submit")
+        self._pending = getattr(self, "_pending", {})
+        self._pending[t.value] = len(wave)
+        return t.value
+
+    def poll(self, timeout_s: float = 0.0):
+        """(ticket, results in packed order, GPU-busy seconds) of the oldest
+        finished submission, or None when nothing finished in time."""
+        pending = getattr(self, "_pending", {})
+        if not pending:
+            return None
+        cap = max(pending.values())
+        out = np.zeros(cap, RESULT_DTYPE)
+        t, n, busy = C.c_uint64(), C.c_size_t(), C.c_double()
+        st = lib().ce_poll(self.handle, int(timeout_s * 1e6), C.byref(t), _ptr(out), cap, C.byref(n), C.byref(busy))
+        if st == CE_ERR_TIMEOUT:
+            return None
+        _check(st, "ce_poll")
+        pending.pop(t.value, None)
+        return t.value, out[:n.value].copy(), busy.value
+
+    def wait(self, timeout_s: float) -> bool:
+        st = lib().ce_wait(self.handle, int(timeout_s * 1e6))
+        if st == CE_ERR_TIMEOUT:
+            return False
+        _check(st, "ce_wait")
+        return True
+
+    def free_slots(self) -> int:
+        return int(lib().ce_free_slots(self.handle))
+
+    def allocated_bytes(self) -> int:
+        return int(lib().ce_allocated_bytes(self.handle))
+
+    def release_idle(self) -> None:
+        _check(lib().ce_release_idle(self.handle), "ce_release_idle")
+
+    def inject_fault(self, after: int, status: int) -> None:
+        _check(lib().ce_inject_fault(self.handle, after, status), "ce_inject_fault")
+
+    def run(self, wave: WavePack, world: World, timeout_s: float = 600.0):
+        """Submit and wait: (results in packed order, busy seconds)."""
+        t = self.submit(wave, world)
+        while True:
+            got = self.poll(timeout_s)
+            if got is None:
+                raise EngineError(CE_ERR_TIMEOUT, "submission did not finish")
+            if got[0] == t:
+                return got[1], got[2]
+
+    def record(self, wave: WavePack, world: World):
+        """Every frame of each creature of `wave` (at most 64): an array
+        [creature, frame, slot, 2] in the reference's frame layout
+        (src/creature_kernel.rs:312-326), and the results in packed order."""
+        k = len(wave)
+        stride = frame_stride(wave.max_muscles)
+        frames_per = settle_frames(world) + trial_steps(world) + 1
+        frames = np.zeros((k, frames_per, stride, 2), np.float32)
+        res = np.zeros(k, RESULT_DTYPE)
+        _check(lib().ce_record(self.handle, C.byref(wave.c()), C.byref(world), _ptr(frames), frames.size,
+                               _ptr(res)), "ce_record")
+        return frames, res
+
+    def scratch_bytes(self, flags: int, rate: int, max_nodes: int, max_muscles: int) -> int:
+        return int(lib().ce_advance_scratch_bytes(self.handle, flags, rate, max_nodes, max_muscles))
+
+    def advance_device(self, records: int, muscles: int, heads: int, results: int, counter: int, scratch: int,
+                       params: Params, flags: int, rate: int, max_nodes: int, max_muscles: int,
+                       stream: int = 0) -> None:
+        """The kernel ABI on device pointers (asynchronous on `stream`)."""
+        _check(lib().ce_advance_device(self.handle, records, muscles, heads, results, counter, scratch,
+                                       C.byref(params), flags, rate, max_nodes, max_muscles, stream or None),
+               "ce_advance_device")
+
+
+def evaluate(engine: Engine, pop: Population, world: World, indices=None) -> np.ndarray:
+    """Results in population (or `indices`) order, as Gpu::evaluate gives them."""
+    wave = pack(pop, world, indices)
+    res, _ = engine.run(wave, world)
+    out = np.zeros(len(wave), RESULT_DTYPE)
+    out[wave.slots] = res
+    return out
+
+
+# ---------------------------------------------------------------- metrics
+def to_metrics(results: np.ndarray, node_counts: np.ndarray, world: World) -> np.ndarray:
+    out = np.zeros(len(results), METRICS_DTYPE)
+    L = lib()
+    res = np.ascontiguousarray(results)
+    for i in range(len(results)):
+        _check(L.ce_to_metrics(res[i:i + 1].ctypes.data, int(node_counts[i]), C.byref(world),
+                               out[i:i + 1].ctypes.data), "ce_to_metrics")
+    return out
+
+
+def niche(pop: Population, i: int, metrics_row: np.ndarray, global_layout: bool = True):
+    """(dense cell index or -1, the six niche bytes) of creature i."""
+    n, _, m, _ = pop.creature(i)
+    nodes = np.ascontiguousarray(n)
+    row = np.ascontiguousarray(np.asarray(metrics_row, METRICS_DTYPE).reshape(1))
+    out = np.zeros(6, np.uint8)
+    cell = lib().ce_niche(nodes.ctypes.data, len(n), len(m), row.ctypes.data, 1 if global_layout else 0,
+                          out.ctypes.data)
+    return int(cell), out

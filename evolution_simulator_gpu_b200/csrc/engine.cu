@@ -1,0 +1,568 @@
+// The engine behind the C ABI: one handle per GPU, a few submission slots,
+// each with its stream, events, pinned staging and device buffers.
+//
+// A submission (the reference's CudaEngine::launch, src/cuda_engine.rs:
+// 2106-2316) uploads the packed batch, splits it into size classes by node
+// count (8, 16 or 32 node rows a lane), runs one persistent launch per class,
+// and reads the results back, all on the slot's stream. ce_poll hands back
+// the oldest finished submission with its GPU-busy seconds, as the
+// reference's poll does (src/cuda_engine.rs:2319-2393).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/creature_engine.h"
+#include "host_model.h"
+#include "kernels.h"
+
+using ce::set_error;
+
+namespace {
+
+constexpr unsigned kClasses[3] = {8u, 16u, 32u};
+
+ce_status cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CE_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return CE_ERR_OOM;
+    }
+    return CE_ERR_DEVICE;
+}
+#define CE_TRY(expr, what)                                   \
+    do {                                                     \
+        ce_status _s = cuda_status((expr), (what));          \
+        if (_s != CE_OK) return _s;                          \
+    } while (0)
+
+// A device buffer that grows and keeps its memory for later submissions.
+struct DeviceBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ce_status ensure(size_t need) {
+        if (need <= bytes) return CE_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grown = std::max(need, (size_t)1 << 20);
+        CE_TRY(cudaMalloc(&ptr, grown), "cudaMalloc");
+        bytes = grown;
+        return CE_OK;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+struct PinnedBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ce_status ensure(size_t need) {
+        if (need <= bytes) return CE_OK;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const size_t grown = std::max(need, (size_t)1 << 20);
+        CE_TRY(cudaMallocHost(&ptr, grown), "cudaMallocHost");
+        bytes = grown;
+        return CE_OK;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct ClassPlan {
+    unsigned ns;
+    uint32_t first, count;  // range of the order list
+    uint32_t mm;            // most muscles in the class
+};
+
+struct Slot {
+    bool busy = false;
+    uint64_t ticket = 0;
+    size_t count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr, done = nullptr;
+    DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_order, d_counters, d_scratch;
+    PinnedBuf h_upload, h_results;
+    std::chrono::steady_clock::time_point submitted;
+};
+
+}  // namespace
+
+struct ce_engine {
+    int device = 0;
+    int sms = 0;
+    unsigned ctas_per_sm = 0;  // 0: from the occupancy of each kernel
+    unsigned chunk_k = 4;
+    std::vector<Slot> slots;
+    std::deque<size_t> pending;  // slot indices, oldest first
+    uint64_t next_ticket = 1;
+    uint32_t fault_after = 0;
+    ce_status fault_status = CE_OK;
+    // Recording buffers.
+    DeviceBuf rec_frames, rec_lanes, rec_muscles, rec_heads, rec_results, rec_counter, rec_scratch;
+};
+
+namespace {
+
+ce_status set_device(ce_engine* e) { return cuda_status(cudaSetDevice(e->device), "cudaSetDevice"); }
+
+// The grid of a persistent launch for a class: every block that fits.
+unsigned grid_for(ce_engine* e, unsigned ns, uint32_t flags, bool record, int rate, size_t count) {
+    int per_sm = 0;
+    if (e->ctas_per_sm) {
+        per_sm = (int)e->ctas_per_sm;
+    } else if (cek::advance_occupancy(ns, flags, record, rate, cek::kBlock, &per_sm) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const size_t needed = (count + cek::kBlock - 1) / cek::kBlock;
+    const size_t full = (size_t)per_sm * (size_t)e->sms;
+    return (unsigned)std::max<size_t>(1, std::min(needed, full));
+}
+
+size_t scratch_bytes(unsigned grid, unsigned ns, unsigned mm, bool record) {
+    const size_t warps = (size_t)grid * (cek::kBlock / 32u);
+    return warps * cek::slot_lines(ns, mm, record) * 32u * 16u;
+}
+
+unsigned class_of_nodes(unsigned n) { return n <= 8 ? 8u : (n <= 16 ? 16u : 32u); }
+
+ce_status check_world(const ce_world* w) {
+    if (!w) {
+        set_error("null world");
+        return CE_ERR_INVALID;
+    }
+    const uint32_t rate = ce::world_rate(*w);
+    if (rate != 60 && rate != 120) {
+        set_error("the engine runs 60 or 120 steps per second");
+        return CE_ERR_UNSUPPORTED;
+    }
+    if (ce::world_steps(*w) < 1) {
+        set_error("a trial needs at least one step");
+        return CE_ERR_INVALID;
+    }
+    return CE_OK;
+}
+
+// Splits the packed batch into size classes: the order list holds the packed
+// positions of each class in turn, each class in packed order.
+ce_status plan_classes(const ce_wave_pack* pack, std::vector<uint32_t>& order, std::vector<ClassPlan>& plans) {
+    order.clear();
+    plans.clear();
+    order.reserve(pack->count);
+    for (unsigned ns : kClasses) {
+        ClassPlan c{ns, (uint32_t)order.size(), 0, 0};
+        for (size_t i = 0; i < pack->count; i++) {
+            const uint32_t* h = pack->heads + 8 * i;
+            const unsigned n = h[0] & 255u, m = h[1];
+            if (n < 2 || n > CE_MAX_NODES || m > CE_MAX_MUSCLES) {
+                set_error("Unsupported body for the CUDA kernel: " + std::to_string(n) + " nodes, " +
+                          std::to_string(m) + " muscles");
+                return CE_ERR_INVALID;
+            }
+            if (class_of_nodes(n) != ns) continue;
+            order.push_back((uint32_t)i);
+            c.mm = std::max(c.mm, m);
+        }
+        c.count = (uint32_t)order.size() - c.first;
+        if (c.count) plans.push_back(c);
+    }
+    return CE_OK;
+}
+
+}  // namespace
+
+extern "C" const char* ce_last_error(void) { return ce::g_last_error.c_str(); }
+
+extern "C" ce_status ce_open(int device, const ce_options* options, ce_engine** out) {
+    if (!out) {
+        set_error("ce_open: null out");
+        return CE_ERR_INVALID;
+    }
+    *out = nullptr;
+    int count = 0;
+    CE_TRY(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (device < 0 || device >= count) {
+        set_error("ce_open: no CUDA device " + std::to_string(device));
+        return CE_ERR_INVALID;
+    }
+    cudaDeviceProp prop;
+    CE_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10) {
+        set_error(std::string("ce_open: the kernels are built for sm_100a, device is ") + prop.name);
+        return CE_ERR_UNSUPPORTED;
+    }
+    ce_engine* e = new ce_engine();
+    e->device = device;
+    e->sms = prop.multiProcessorCount;
+    unsigned nslots = 4;
+    if (options) {
+        if (options->slots) nslots = options->slots;
+        e->ctas_per_sm = options->ctas_per_sm;
+    }
+    ce_status s = set_device(e);
+    if (s != CE_OK) {
+        delete e;
+        return s;
+    }
+    e->slots.resize(nslots);
+    for (Slot& sl : e->slots) {
+        s = cuda_status(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.start), "cudaEventCreate");
+        if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.stop), "cudaEventCreate");
+        if (s == CE_OK) s = cuda_status(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "cudaEventCreate");
+        if (s != CE_OK) {
+            ce_close(e);
+            return s;
+        }
+    }
+    *out = e;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_close(ce_engine* e) {
+    if (!e) return CE_OK;
+    cudaSetDevice(e->device);
+    for (Slot& sl : e->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        sl.d_lanes.release();
+        sl.d_muscles.release();
+        sl.d_heads.release();
+        sl.d_results.release();
+        sl.d_order.release();
+        sl.d_counters.release();
+        sl.d_scratch.release();
+        sl.h_upload.release();
+        sl.h_results.release();
+        if (sl.start) cudaEventDestroy(sl.start);
+        if (sl.stop) cudaEventDestroy(sl.stop);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    e->rec_frames.release();
+    e->rec_lanes.release();
+    e->rec_muscles.release();
+    e->rec_heads.release();
+    e->rec_results.release();
+    e->rec_counter.release();
+    e->rec_scratch.release();
+    delete e;
+    return CE_OK;
+}
+
+extern "C" int ce_free_slots(ce_engine* e) {
+    if (!e) return 0;
+    int n = 0;
+    for (const Slot& sl : e->slots) n += sl.busy ? 0 : 1;
+    return n;
+}
+
+extern "C" size_t ce_allocated_bytes(ce_engine* e) {
+    if (!e) return 0;
+    size_t b = e->rec_frames.bytes + e->rec_lanes.bytes + e->rec_muscles.bytes + e->rec_heads.bytes +
+               e->rec_results.bytes + e->rec_counter.bytes + e->rec_scratch.bytes;
+    for (const Slot& sl : e->slots) {
+        b += sl.d_lanes.bytes + sl.d_muscles.bytes + sl.d_heads.bytes + sl.d_results.bytes + sl.d_order.bytes +
+             sl.d_counters.bytes + sl.d_scratch.bytes;
+    }
+    return b;
+}
+
+extern "C" ce_status ce_release_idle(ce_engine* e) {
+    if (!e) return CE_ERR_INVALID;
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    for (Slot& sl : e->slots) {
+        if (sl.busy) continue;
+        sl.d_lanes.release();
+        sl.d_muscles.release();
+        sl.d_heads.release();
+        sl.d_results.release();
+        sl.d_order.release();
+        sl.d_counters.release();
+        sl.d_scratch.release();
+        sl.h_upload.release();
+        sl.h_results.release();
+    }
+    return CE_OK;
+}
+
+extern "C" ce_status ce_inject_fault(ce_engine* e, uint32_t after, ce_status status) {
+    if (!e) return CE_ERR_INVALID;
+    e->fault_after = after;
+    e->fault_status = status;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_world* w, uint64_t* ticket) {
+    if (!e || !pack || !ticket || (pack->count && (!pack->lanes || !pack->muscles || !pack->heads))) {
+        set_error("ce_submit: null argument");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = check_world(w);
+    if (s != CE_OK) return s;
+    if (e->fault_after) {
+        if (--e->fault_after == 0) {
+            set_error("ce_submit: injected fault");
+            return e->fault_status;
+        }
+    }
+    size_t si = e->slots.size();
+    for (size_t i = 0; i < e->slots.size(); i++) {
+        if (!e->slots[i].busy) {
+            si = i;
+            break;
+        }
+    }
+    if (si == e->slots.size()) {
+        set_error("ce_submit: no free slot");
+        return CE_ERR_BUSY;
+    }
+    Slot& sl = e->slots[si];
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    std::vector<uint32_t> order;
+    std::vector<ClassPlan> plans;
+    if ((s = plan_classes(pack, order, plans)) != CE_OK) return s;
+    const uint32_t flags = ce_world_flags(w);
+    const int rate = (int)ce::world_rate(*w);
+    ce_params p;
+    ce_make_params(w, 0, (uint32_t)pack->count, 0, &p);
+    // Grids and scratch of the classes, which run one after another on the
+    // slot's stream and share its scratch.
+    std::vector<unsigned> grids(plans.size());
+    size_t scratch = 0;
+    for (size_t c = 0; c < plans.size(); c++) {
+        grids[c] = grid_for(e, plans[c].ns, flags, false, rate, plans[c].count);
+        scratch = std::max(scratch, scratch_bytes(grids[c], plans[c].ns, plans[c].mm, false));
+    }
+    const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
+    const size_t order_b = order.size() * 4, res_b = pack->count * sizeof(ce_result);
+    if ((s = sl.d_lanes.ensure(lanes_b)) || (s = sl.d_muscles.ensure(mus_b)) || (s = sl.d_heads.ensure(heads_b)) ||
+        (s = sl.d_order.ensure(std::max<size_t>(order_b, 4))) || (s = sl.d_results.ensure(res_b)) ||
+        (s = sl.d_counters.ensure(64)) || (s = sl.d_scratch.ensure(scratch)) ||
+        (s = sl.h_upload.ensure(lanes_b + mus_b + heads_b + order_b)) || (s = sl.h_results.ensure(res_b))) {
+        return s;
+    }
+    // Stage the batch in pinned memory, then copy it up asynchronously.
+    char* up = static_cast<char*>(sl.h_upload.ptr);
+    std::memcpy(up, pack->lanes, lanes_b);
+    std::memcpy(up + lanes_b, pack->muscles, mus_b);
+    std::memcpy(up + lanes_b + mus_b, pack->heads, heads_b);
+    if (order_b) std::memcpy(up + lanes_b + mus_b + heads_b, order.data(), order_b);
+    cudaStream_t st = sl.stream;
+    CE_TRY(cudaMemcpyAsync(sl.d_lanes.ptr, up, lanes_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    CE_TRY(cudaMemcpyAsync(sl.d_muscles.ptr, up + lanes_b, mus_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    CE_TRY(cudaMemcpyAsync(sl.d_heads.ptr, up + lanes_b + mus_b, heads_b, cudaMemcpyHostToDevice, st),
+           "cudaMemcpyAsync");
+    if (order_b) {
+        CE_TRY(cudaMemcpyAsync(sl.d_order.ptr, up + lanes_b + mus_b + heads_b, order_b, cudaMemcpyHostToDevice, st),
+               "cudaMemcpyAsync");
+    }
+    CE_TRY(cudaMemsetAsync(sl.d_counters.ptr, 0, 64, st), "cudaMemsetAsync");
+    CE_TRY(cudaEventRecord(sl.start, st), "cudaEventRecord");
+    for (size_t c = 0; c < plans.size(); c++) {
+        cek::KernelArgs a{};
+        a.records = static_cast<const uint32_t*>(sl.d_lanes.ptr);
+        a.muscles = static_cast<const float*>(sl.d_muscles.ptr);
+        a.heads = static_cast<const uint4*>(sl.d_heads.ptr);
+        a.results = static_cast<ce_result*>(sl.d_results.ptr);
+        a.counter = static_cast<uint32_t*>(sl.d_counters.ptr) + c;
+        a.scratch = static_cast<float4*>(sl.d_scratch.ptr);
+        a.frames = nullptr;
+        a.order = static_cast<const uint32_t*>(sl.d_order.ptr) + plans[c].first;
+        a.count = plans[c].count;
+        a.mm = plans[c].mm;
+        a.frames_per_creature = 0;
+        a.chunk_k = e->chunk_k;
+        cek::LaunchSpec ls{plans[c].ns, flags, false, rate, grids[c], cek::kBlock, st};
+        CE_TRY(cek::launch_advance(ls, a, p), "advance launch");
+    }
+    CE_TRY(cudaEventRecord(sl.stop, st), "cudaEventRecord");
+    CE_TRY(cudaMemcpyAsync(sl.h_results.ptr, sl.d_results.ptr, res_b, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CE_TRY(cudaEventRecord(sl.done, st), "cudaEventRecord");
+    sl.busy = true;
+    sl.count = pack->count;
+    sl.ticket = e->next_ticket++;
+    sl.submitted = std::chrono::steady_clock::now();
+    e->pending.push_back(si);
+    *ticket = sl.ticket;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_wait(ce_engine* e, int64_t timeout_us) {
+    if (!e) return CE_ERR_INVALID;
+    if (e->pending.empty()) return CE_ERR_TIMEOUT;
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds(std::max<int64_t>(timeout_us, 0));
+    for (;;) {
+        for (size_t si : e->pending) {
+            const cudaError_t q = cudaEventQuery(e->slots[si].done);
+            if (q == cudaSuccess) return CE_OK;
+            if (q != cudaErrorNotReady) return cuda_status(q, "cudaEventQuery");
+        }
+        if (timeout_us >= 0 && std::chrono::steady_clock::now() >= deadline) return CE_ERR_TIMEOUT;
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
+extern "C" ce_status ce_poll(ce_engine* e, int64_t timeout_us, uint64_t* ticket, ce_result* out, size_t cap,
+                             size_t* n, double* busy_seconds) {
+    if (!e || !ticket || !n) {
+        set_error("ce_poll: null argument");
+        return CE_ERR_INVALID;
+    }
+    *n = 0;
+    if (e->pending.empty()) {
+        set_error("ce_poll: nothing in flight");
+        return CE_ERR_TIMEOUT;
+    }
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    const size_t si = e->pending.front();
+    Slot& sl = e->slots[si];
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds(std::max<int64_t>(timeout_us, 0));
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(sl.done);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) return cuda_status(q, "cudaEventQuery");
+        if (timeout_us >= 0 && std::chrono::steady_clock::now() >= deadline) {
+            set_error("ce_poll: timeout");
+            return CE_ERR_TIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+    if (out && cap < sl.count) {
+        set_error("ce_poll: result buffer too small");
+        return CE_ERR_INVALID;
+    }
+    float ms = 0.0f;
+    CE_TRY(cudaEventElapsedTime(&ms, sl.start, sl.stop), "cudaEventElapsedTime");
+    if (out) std::memcpy(out, sl.h_results.ptr, sl.count * sizeof(ce_result));
+    *ticket = sl.ticket;
+    *n = sl.count;
+    if (busy_seconds) *busy_seconds = ms * 1e-3;
+    sl.busy = false;
+    e->pending.pop_front();
+    return CE_OK;
+}
+
+extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_world* w, float* frames,
+                               size_t frames_cap_floats, ce_result* results) {
+    if (!e || !pack || !frames || !results || !pack->count) {
+        set_error("ce_record: null argument or empty batch");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = check_world(w);
+    if (s != CE_OK) return s;
+    if (pack->count > 64) {
+        set_error("ce_record: at most 64 creatures a recording");
+        return CE_ERR_INVALID;
+    }
+    std::vector<uint32_t> order;
+    std::vector<ClassPlan> plans;
+    if ((s = plan_classes(pack, order, plans)) != CE_OK) return s;
+    unsigned ns = 8, mm = 0;
+    for (const ClassPlan& c : plans) {
+        ns = std::max(ns, c.ns);
+        mm = std::max(mm, c.mm);
+    }
+    const uint32_t flags = ce_world_flags(w);
+    const int rate = (int)ce::world_rate(*w);
+    const uint32_t stride = ce_frame_stride(mm);
+    ce_params p;
+    ce_make_params(w, 0, (uint32_t)pack->count, stride, &p);
+    const uint32_t per = ce::world_settle(*w) + p.steps + 1u;
+    const size_t frame_floats = (size_t)pack->count * per * stride * 2u;
+    if (frames_cap_floats < frame_floats) {
+        set_error("ce_record: frame buffer too small, need " + std::to_string(frame_floats) + " floats");
+        return CE_ERR_INVALID;
+    }
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    const unsigned grid = 1;
+    const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
+    const size_t res_b = pack->count * sizeof(ce_result);
+    if ((s = e->rec_frames.ensure(frame_floats * 4)) || (s = e->rec_lanes.ensure(lanes_b)) ||
+        (s = e->rec_muscles.ensure(mus_b)) || (s = e->rec_heads.ensure(heads_b)) || (s = e->rec_results.ensure(res_b)) ||
+        (s = e->rec_counter.ensure(4)) || (s = e->rec_scratch.ensure(scratch_bytes(grid, ns, mm, true)))) {
+        return s;
+    }
+    CE_TRY(cudaMemcpy(e->rec_lanes.ptr, pack->lanes, lanes_b, cudaMemcpyHostToDevice), "cudaMemcpy");
+    CE_TRY(cudaMemcpy(e->rec_muscles.ptr, pack->muscles, mus_b, cudaMemcpyHostToDevice), "cudaMemcpy");
+    CE_TRY(cudaMemcpy(e->rec_heads.ptr, pack->heads, heads_b, cudaMemcpyHostToDevice), "cudaMemcpy");
+    CE_TRY(cudaMemset(e->rec_counter.ptr, 0, 4), "cudaMemset");
+    CE_TRY(cudaMemset(e->rec_frames.ptr, 0, frame_floats * 4), "cudaMemset");
+    cek::KernelArgs a{};
+    a.records = static_cast<const uint32_t*>(e->rec_lanes.ptr);
+    a.muscles = static_cast<const float*>(e->rec_muscles.ptr);
+    a.heads = static_cast<const uint4*>(e->rec_heads.ptr);
+    a.results = static_cast<ce_result*>(e->rec_results.ptr);
+    a.counter = static_cast<uint32_t*>(e->rec_counter.ptr);
+    a.scratch = static_cast<float4*>(e->rec_scratch.ptr);
+    a.frames = static_cast<float2*>(e->rec_frames.ptr);
+    a.order = nullptr;
+    a.count = (uint32_t)pack->count;
+    a.mm = mm;
+    a.frames_per_creature = per;
+    a.chunk_k = 1;
+    cek::LaunchSpec ls{ns, flags, true, rate, grid, cek::kBlock, nullptr};
+    CE_TRY(cek::launch_advance(ls, a, p), "record launch");
+    CE_TRY(cudaDeviceSynchronize(), "record kernel");
+    CE_TRY(cudaMemcpy(frames, e->rec_frames.ptr, frame_floats * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    CE_TRY(cudaMemcpy(results, e->rec_results.ptr, res_b, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CE_OK;
+}
+
+extern "C" size_t ce_advance_scratch_bytes(ce_engine* e, uint32_t world_flags, uint32_t rate, uint32_t max_nodes,
+                                           uint32_t max_muscles) {
+    if (!e || max_nodes < 2 || max_nodes > CE_MAX_NODES || max_muscles > CE_MAX_MUSCLES) return 0;
+    if (rate != 60 && rate != 120) return 0;
+    const unsigned ns = class_of_nodes(max_nodes);
+    const unsigned grid = grid_for(e, ns, world_flags, false, (int)rate, (size_t)1 << 30);
+    return scratch_bytes(grid, ns, max_muscles, false);
+}
+
+extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, const float* muscles,
+                                       const uint32_t* heads, ce_result* results, uint32_t* counter, void* scratch,
+                                       const ce_params* params, uint32_t world_flags, uint32_t rate,
+                                       uint32_t max_nodes, uint32_t max_muscles, void* stream) {
+    if (!e || !records || !muscles || !heads || !results || !counter || !scratch || !params) {
+        set_error("ce_advance_device: null argument");
+        return CE_ERR_INVALID;
+    }
+    if (max_nodes < 2 || max_nodes > CE_MAX_NODES || max_muscles > CE_MAX_MUSCLES || params->steps < 1 ||
+        (rate != 60 && rate != 120)) {
+        set_error("ce_advance_device: unsupported sizes");
+        return CE_ERR_INVALID;
+    }
+    CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    const unsigned ns = class_of_nodes(max_nodes);
+    const unsigned grid = grid_for(e, ns, world_flags, false, (int)rate, params->count);
+    cek::KernelArgs a{};
+    a.records = records;
+    a.muscles = muscles;
+    a.heads = reinterpret_cast<const uint4*>(heads);
+    a.results = results;
+    a.counter = counter;
+    a.scratch = static_cast<float4*>(scratch);
+    a.frames = nullptr;
+    a.order = nullptr;
+    a.count = params->count;
+    a.mm = max_muscles;
+    a.frames_per_creature = 0;
+    a.chunk_k = e->chunk_k;
+    cek::LaunchSpec ls{ns, world_flags, false, (int)rate, grid, cek::kBlock, static_cast<cudaStream_t>(stream)};
+    CE_TRY(cek::launch_advance(ls, a, *params), "advance launch");
+    return CE_OK;
+}

@@ -1,0 +1,61 @@
+// Launch interface of the creature kernel family, shared by the kernels and
+// the host engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/creature_engine.h"
+
+namespace cek {
+
+// Threads per block and the blocks per multiprocessor the register budget
+// is sized for (128 registers a thread at most).
+constexpr unsigned kBlock = 128;
+constexpr unsigned kMinBlocks = 4;
+
+// Worlds compiled with their effects fixed: the calm world, the effects
+// world (rough ground, slope, hurdles, water, ice, wind, thick air), the
+// same with earthquakes, and every effect on. Other worlds run on the kernel
+// that reads the switches at run time.
+constexpr uint32_t kWorldCalm = CE_FLAG_GROUND;
+constexpr uint32_t kWorldEffects = CE_FLAG_GROUND | CE_FLAG_TERRAIN | CE_FLAG_SLOPE | CE_FLAG_HURDLES |
+                                   CE_FLAG_WATER | CE_FLAG_ICE | CE_FLAG_WIND | CE_FLAG_AIR;
+constexpr uint32_t kWorldEffectsQuake = kWorldEffects | CE_FLAG_QUAKE;
+constexpr uint32_t kWorldAll = 0xfffu;
+
+// Shared memory of a block: the position/velocity table (16 bytes) and the
+// force table (8 bytes) for `ns` node rows of every thread.
+inline size_t smem_bytes(unsigned ns, unsigned block) { return (size_t)ns * block * 24u; }
+
+struct KernelArgs {
+    const uint32_t* records;
+    const float* muscles;
+    const uint4* heads;
+    ce_result* results;
+    uint32_t* counter;
+    float4* scratch;               // slots: warps of the grid x lines x 32 lanes
+    float2* frames;                // RECORD: frames of each recorded creature
+    const uint32_t* order;         // packed positions of this launch's creatures
+    uint32_t count;                // creatures of this launch
+    uint32_t mm;                   // most muscles of a body of this launch
+    uint32_t frames_per_creature;  // RECORD: frames of one recording
+    uint32_t chunk_k;              // claims shrink to 1 / chunk_k of the rest per warp
+};
+
+struct LaunchSpec {
+    unsigned ns;     // node rows: 8, 16 or 32
+    uint32_t flags;  // world effect bits
+    bool record;
+    int rate;        // steps per second: 60 or 120
+    unsigned grid, block;
+    cudaStream_t stream;
+};
+
+// 16-byte lines of one lane's slot for a class.
+unsigned slot_lines(unsigned ns, unsigned mm, bool record);
+
+cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
+cudaError_t advance_occupancy(unsigned ns, uint32_t flags, bool record, int rate, unsigned block, int* blocks);
+
+}  // namespace cek

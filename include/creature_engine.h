@@ -1,0 +1,294 @@
+/*
+ * creature_engine.h -- C ABI of the B200 creature-evaluation engine.
+ *
+ * The engine runs whole creature trials (the position-based-dynamics substep
+ * loop, its per-step tallies, the early rungs and the screen) on an sm_100a
+ * GPU and returns one result record per creature. It replaces the CUDA
+ * backend and engine thread of the evolution simulator:
+ *
+ *   reference (Rust)                                   this header
+ *   ----------------------------------------------------------------------
+ *   shaders/creature.cu:1266-1277  advance(...)        ce_advance_device
+ *   src/cuda_engine.rs:2106-2316   CudaEngine::launch  ce_submit
+ *   src/cuda_engine.rs:2319-2393   CudaEngine::poll    ce_poll
+ *   src/cuda_engine.rs:2054-2100   CudaEngine::record  ce_record
+ *   src/engine.rs:163-199          trait Engine        ce_open/ce_submit/
+ *                                                      ce_poll/ce_wait/
+ *                                                      ce_free_slots/
+ *                                                      ce_allocated_bytes
+ *   src/engine.rs:430-469          trait Device        ce_release_idle
+ *   src/kernel.rs:471-593          pack_reusing        ce_pack
+ *   src/kernel.rs:212-251          params              ce_make_params
+ *   src/kernel.rs:82-106           world_flags         ce_world_flags
+ *   src/scheduler.rs:859-923       trial_steps/to_metrics  ce_to_metrics
+ *   src/qd.rs:762-846, 988-999     descriptor/niche_in/cell_index ce_niche
+ *
+ * Every struct below that the reference also defines has the reference's
+ * field order and size, so the reference's #[repr(C)] buffers (WavePack
+ * words, Params, GpuResult, NodeGene, Bone, Muscle) pass through unchanged.
+ *
+ * Errors: every entry point returns a ce_status. CE_ERR_OOM is the
+ * out-of-memory case the reference's MemoryBackoff retries
+ * (src/cuda_engine.rs:425-448, src/engine.rs:534-650); CE_ERR_DEVICE means
+ * the engine must be closed and opened again (src/scheduler.rs:742-806).
+ * ce_last_error() gives a thread-local message for the last failure.
+ *
+ * Threading: one handle per GPU, used from one thread at a time, like the
+ * reference's engine thread (src/engine.rs:656-719).
+ */
+#ifndef CREATURE_ENGINE_H
+#define CREATURE_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum ce_status {
+    CE_OK = 0,
+    CE_ERR_INVALID = 1,     /* bad argument, unsupported body or size      */
+    CE_ERR_OOM = 2,         /* device or pinned memory exhausted           */
+    CE_ERR_TIMEOUT = 3,     /* nothing finished within the timeout         */
+    CE_ERR_DEVICE = 4,      /* CUDA failure: close and reopen the engine   */
+    CE_ERR_UNSUPPORTED = 5, /* no kernel for this request                  */
+    CE_ERR_BUSY = 6         /* no free slot for another submission         */
+} ce_status;
+
+/* ---- layout constants (src/kernel.rs:24-51) ---------------------------- */
+#define CE_MAX_NODES 32
+#define CE_MAX_MUSCLES 96
+#define CE_NODE_WORDS 6
+#define CE_BONE_WORDS 6
+#define CE_MUSCLE_FIELDS 20
+#define CE_SUBSTEPS 16
+#define CE_WAVE 262144
+#define CE_NO_SENSOR 255u   /* src/evolution.rs:247 */
+#define CE_NONE 0xffffffffu /* no parent bone / no sensor in the records */
+
+/* World effect bits of ce_world_flags (src/kernel.rs:82-113). */
+#define CE_FLAG_GROUND (1u << 0)
+#define CE_FLAG_TERRAIN (1u << 1)
+#define CE_FLAG_SLOPE (1u << 2)
+#define CE_FLAG_GAPS (1u << 3)
+#define CE_FLAG_HURDLES (1u << 4)
+#define CE_FLAG_QUAKE (1u << 5)
+#define CE_FLAG_MUD (1u << 6)
+#define CE_FLAG_WATER (1u << 7)
+#define CE_FLAG_ICE (1u << 8)
+#define CE_FLAG_WIND (1u << 9)
+#define CE_FLAG_AIR (1u << 10)
+#define CE_FLAG_BRAMBLES (1u << 11)
+
+/* ---- genes (src/evolution.rs:41-50, 58-80, 209-243) -------------------- */
+typedef struct ce_node_gene {
+    float x, y, diameter, friction;
+} ce_node_gene;
+
+typedef struct ce_bone_gene {
+    uint32_t a, b;
+    float rest_length, min_angle, max_angle, organ_mass, organ_at;
+} ce_bone_gene;
+
+typedef struct ce_muscle_gene {
+    uint32_t bone_a, bone_b;
+    float anchor_a, anchor_b;
+    float short_len, long_len; /* `short` and `long` in the reference */
+    float period, phase, duty, stiffness;
+    uint32_t sensor;
+    float reset, tendon;
+} ce_muscle_gene;
+
+/* One creature of an arena-packed population (src/evolution.rs:254-269,
+ * 440-453): the ranges of its genes in the three gene arrays and its id. */
+typedef struct ce_genome {
+    uint32_t node_start, node_count;
+    uint32_t bone_start, bone_count;
+    uint32_t muscle_start, muscle_count;
+    uint64_t id;
+    uint32_t flags; /* rungs::AUDIT and the others (src/rungs.rs:18-35) */
+    uint32_t reserved;
+} ce_genome;
+
+typedef struct ce_population {
+    const ce_node_gene* nodes;
+    const ce_bone_gene* bones;
+    const ce_muscle_gene* muscles;
+    const ce_genome* genomes;
+    size_t count;
+    /* Optional factor on each muscle's strength (one per muscle gene, NULL
+     * for 1): it multiplies the force cap and the energy store, as the
+     * reference's `muscle_scale` does (src/kernel.rs:376, 390-391). */
+    const float* strength_scale;
+} ce_population;
+
+/* ---- world (the physics subset of src/config.rs:119-161) --------------- */
+typedef struct ce_rung {
+    float w[6];
+    float bias;
+    uint32_t off;
+} ce_rung; /* rungs::Rung, shaders/creature.cu:66-70 */
+
+typedef struct ce_world {
+    uint32_t ground;    /* bool */
+    uint32_t terrain;   /* roughness level, 0..4 (physics.rs:523-527) */
+    float gravity, air_retention, ground_friction;
+    float muscle_energy, muscle_recovery;
+    float slope, wind, mud, brambles, water, patches, gaps, hurdles, quake;
+    float duration;     /* seconds */
+    uint32_t rate;      /* steps per second: 60 standard, 120 fine */
+    uint32_t has_screen;
+    float screen_seconds, screen_bar, screen_bar_young, screen_bar_reshaped;
+    uint32_t has_rungs;
+    ce_rung rungs[2];
+} ce_world;
+
+/* ---- kernel ABI (shaders/creature.cu:75-128) --------------------------- */
+typedef struct ce_params {
+    uint32_t count, base, steps, screen_step, stride;
+    float gravity, air, friction, terrain, muscle_energy, muscle_recovery;
+    float slope, wind, mud, gaps, hurdles, quake;
+    float screen_bar, screen_bar_young, screen_bar_reshaped;
+    float water, patches, air_sub, inv_muscle_energy, brambles;
+    ce_rung r1, r2;
+} ce_params;
+
+typedef struct ce_result {
+    float fitness, ground_contact, vertical_oscillation, gait_frequency;
+    float previous_center_y, vertical_extremum, vertical_trend, gait_turns;
+    float height_sum, contact_lo, contact_hi, lift_lo, lift_hi;
+    float ground_lo, ground_hi, fall_time, head_shake, screen_x, screened;
+} ce_result;
+
+/* The packed records of a batch (src/kernel.rs:56-72): node and bone words,
+ * muscle records and two head words (uint32_t[4] each) per creature, in
+ * packed order, which is sorted by (muscles, nodes, population index). */
+typedef struct ce_wave_pack {
+    const uint32_t* lanes;
+    size_t lanes_len; /* words */
+    const float* muscles;
+    size_t muscles_len; /* floats */
+    const uint32_t* heads; /* 8 words per creature */
+    size_t count;          /* creatures */
+} ce_wave_pack;
+
+/* ---- packing (host) ---------------------------------------------------- */
+/* The world's effect bits (src/kernel.rs:82-106). */
+uint32_t ce_world_flags(const ce_world* world);
+
+/* The launch parameters of a wave (src/kernel.rs:212-251). */
+ce_status ce_make_params(const ce_world* world, uint32_t base, uint32_t count, uint32_t stride,
+                         ce_params* out);
+
+/* Sizes of the packed records of `indices` (NULL: every creature). */
+ce_status ce_pack_size(const ce_population* pop, const uint32_t* indices, size_t n,
+                       size_t* lanes_len, size_t* muscles_len);
+
+/* Packs creatures into caller buffers sized by ce_pack_size
+ * (src/kernel.rs:336-411, 471-593). `slots` receives, for each packed
+ * creature, its position in `indices`. `info` (optional, 4 words per
+ * creature) receives node, bone, muscle count and quake hash. */
+ce_status ce_pack(const ce_population* pop, const uint32_t* indices, size_t n, const ce_world* world,
+                  uint32_t* lanes, float* muscles, uint32_t* heads, uint32_t* slots, uint32_t* info);
+
+/* Frame slots of a recording (src/creature_kernel.rs:312-326). */
+uint32_t ce_frame_stride(uint32_t max_muscles);
+
+/* ---- synthetic population generator ------------------------------------ */
+typedef struct ce_gen_spec {
+    uint64_t seed;
+    uint32_t min_nodes, max_nodes;
+    uint32_t node_dist;      /* 0 uniform, 1 geometric with mean `mean_nodes` */
+    float mean_nodes;
+    uint32_t min_muscles, max_muscles;
+    uint32_t muscle_rule;    /* 0 spanning + up to `max_extra` extras,
+                                1 muscle count uniform in [min, max]        */
+    uint32_t max_extra;
+    float joint_lo_deg, joint_hi_deg; /* joint half-range drawn uniformly */
+    float friction_lo, friction_hi;
+    uint64_t first_id;
+} ce_gen_spec;
+
+/* Counts of the genes that ce_generate writes for `count` creatures. */
+ce_status ce_generate_size(const ce_gen_spec* spec, size_t count, size_t* nodes, size_t* bones,
+                           size_t* muscles);
+/* Writes `count` creatures: creature i is a function of (seed, first + i). */
+ce_status ce_generate(const ce_gen_spec* spec, size_t first, size_t count, ce_node_gene* nodes,
+                      ce_bone_gene* bones, ce_muscle_gene* muscles, float* strength_scale,
+                      ce_genome* genomes);
+
+/* ---- metrics (host) ---------------------------------------------------- */
+typedef struct ce_metrics {
+    float fitness, ground_contact, vertical_oscillation, gait_frequency, mean_height, feet;
+    float screen_x;
+    uint32_t screened, steps;
+} ce_metrics;
+
+/* scheduler::to_metrics for one result (src/scheduler.rs:859-923). */
+ce_status ce_to_metrics(const ce_result* r, uint32_t node_count, const ce_world* world,
+                        ce_metrics* out);
+/* qd::descriptor + Descriptor::niche_in + cell_index (src/qd.rs:762-846,
+ * 988-999): the dense cell of a creature in the global (global != 0) or
+ * island layout, -1 outside the grid. */
+int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint32_t muscle_count,
+                 const ce_metrics* m, int global_layout, uint8_t niche_out[6]);
+
+/* ---- engine ------------------------------------------------------------ */
+typedef struct ce_engine ce_engine;
+
+typedef struct ce_options {
+    uint32_t slots;          /* concurrent submissions, 0 = default (4) */
+    uint32_t ctas_per_sm;    /* 0 = autotuned */
+    uint32_t warps_per_cta;  /* 0 = autotuned */
+    uint32_t reserved[5];
+} ce_options;
+
+ce_status ce_open(int device, const ce_options* options, ce_engine** out);
+ce_status ce_close(ce_engine* engine);
+const char* ce_last_error(void);
+
+/* Queues the batch `pack` in world `world` (host memory; copied before the
+ * call returns). Results come back in packed order through ce_poll. */
+ce_status ce_submit(ce_engine* engine, const ce_wave_pack* pack, const ce_world* world,
+                    uint64_t* ticket);
+/* Takes the oldest finished submission. `n` receives its result count;
+ * `cap` must be at least that. CE_ERR_TIMEOUT when none finishes in time. */
+ce_status ce_poll(ce_engine* engine, int64_t timeout_us, uint64_t* ticket, ce_result* out,
+                  size_t cap, size_t* n, double* busy_seconds);
+/* Waits until a submission has finished or `timeout_us` passed. */
+ce_status ce_wait(ce_engine* engine, int64_t timeout_us);
+int ce_free_slots(ce_engine* engine);
+size_t ce_allocated_bytes(ce_engine* engine);
+ce_status ce_release_idle(ce_engine* engine);
+
+/* Records K creatures of `pack` (K = pack->count <= 64): every frame of
+ * each trial, frame-major, `stride` float2 slots per creature and frame
+ * (src/creature_kernel.rs:312-326); frames = SETTLE + steps + 1. Synchronous. */
+ce_status ce_record(ce_engine* engine, const ce_wave_pack* pack, const ce_world* world,
+                    float* frames, size_t frames_cap_floats, ce_result* results);
+
+/* Device-level entry, the kernel ABI of shaders/creature.cu:1266-1277: runs
+ * `params->count` creatures from `params->base` of device-resident records
+ * on `stream` (a cudaStream_t, NULL for the legacy stream). `rate` is the
+ * step rate the reference compiles into its kernel (60 or 120). Bodies must
+ * have at most `max_nodes` nodes and `max_muscles` muscles. `scratch` is a
+ * device buffer of at least ce_advance_scratch_bytes() bytes, `counter`
+ * a device word set to 0 before the call. Asynchronous. */
+size_t ce_advance_scratch_bytes(ce_engine* engine, uint32_t world_flags, uint32_t rate,
+                                uint32_t max_nodes, uint32_t max_muscles);
+ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const float* muscles,
+                            const uint32_t* heads, ce_result* results, uint32_t* counter,
+                            void* scratch, const ce_params* params, uint32_t world_flags,
+                            uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
+                            void* stream);
+
+/* Host-side fault injection for the recovery paths (src/scheduler.rs:725):
+ * the `after`-th next submit fails with `status`. 0 turns it off. */
+ce_status ce_inject_fault(ce_engine* engine, uint32_t after, ce_status status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CREATURE_ENGINE_H */

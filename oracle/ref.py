@@ -1,0 +1,72 @@
+"""Test infrastructure: bindings of the checkers in oracle/_ref/.
+
+* ``RefKernel`` runs the reference's own kernel (shaders/creature.cu, built
+  by oracle/build_ref.py) on the GPU with the reference engine's launch rule.
+  It is the bit-level oracle for the engine's kernel and the GPU baseline.
+* ``Oracle`` runs the CPU restatement of the kernel (oracle/creature_oracle.cpp).
+
+Only tests/, the smoke check and the benchmark's reference arm use this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE / "_ref"
+
+RESULT_DTYPE = np.dtype([(n, "<f4") for n in [
+    "fitness", "ground_contact", "vertical_oscillation", "gait_frequency", "previous_center_y",
+    "vertical_extremum", "vertical_trend", "gait_turns", "height_sum", "contact_lo", "contact_hi", "lift_lo",
+    "lift_hi", "ground_lo", "ground_hi", "fall_time", "head_shake", "screen_x", "screened"]])
+
+
+def variant_path(flags: int, rate: int = 60, record: bool = False) -> Path:
+    return REF / f"libref_{flags:03x}_{rate}_{int(record)}.so"
+
+
+class RefKernel:
+    """The reference kernel for one world, step rate and recording switch."""
+
+    def __init__(self, flags: int, rate: int = 60, record: bool = False):
+        path = variant_path(flags, rate, record)
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is missing: build it with python oracle/build_ref.py")
+        self.lib = C.CDLL(str(path))
+        self.lib.ref_run.restype = C.c_int
+        self.lib.ref_run.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_float),
+                                     C.c_char_p, C.c_size_t]
+        assert self.lib.ref_result_size() == RESULT_DTYPE.itemsize
+        self.params_size = self.lib.ref_params_size()
+        self.record = record
+
+    def run(self, wave, params):
+        """(results in packed order, GPU milliseconds) for the packed batch."""
+        assert C.sizeof(params) == self.params_size, (C.sizeof(params), self.params_size)
+        n = len(wave)
+        out = np.zeros(n, RESULT_DTYPE)
+        ms = C.c_float()
+        err = C.create_string_buffer(512)
+        rc = self.lib.ref_run(wave.lanes.ctypes.data, len(wave.lanes), wave.muscles.ctypes.data,
+                              len(wave.muscles), wave.heads.ctypes.data, n, C.byref(params), out.ctypes.data,
+                              None, 0, C.byref(ms), err, 512)
+        if rc != 0:
+            raise RuntimeError(f"reference kernel failed: {err.value.decode()}")
+        return out, ms.value
+
+    def record_one(self, wave1, params, frames: int, stride: int):
+        """Every frame of the one creature of `wave1`: [frame, slot, 2]."""
+        assert len(wave1) == 1
+        out = np.zeros(1, RESULT_DTYPE)
+        fr = np.zeros((frames, stride, 2), np.float32)
+        ms = C.c_float()
+        err = C.create_string_buffer(512)
+        rc = self.lib.ref_run(wave1.lanes.ctypes.data, len(wave1.lanes), wave1.muscles.ctypes.data,
+                              len(wave1.muscles), wave1.heads.ctypes.data, 1, C.byref(params), out.ctypes.data,
+                              fr.ctypes.data, fr.size, C.byref(ms), err, 512)
+        if rc != 0:
+            raise RuntimeError(f"reference kernel failed: {err.value.decode()}")
+        return fr, out
