@@ -1,0 +1,396 @@
+"""Benchmark: creature-substeps per second at game scale.
+
+Workload (per GPU): one generation of 3,000,000 seeded synthetic creatures
+(seed 1, 3-10 nodes, 2-24 muscles, calm world) in 20 s trials at 60 steps a
+second and 16 substeps a step. A step of the benchmark evaluates the whole
+generation. A creature-substep is one substep of one creature until its trial
+ends (fall, screen or last step), as the reference counts creature-steps
+(examples/p2_speed.rs:55-72) times 16.
+
+Printed, one JSON line from rank 0:
+  value   -- creature-substeps/s of all ranks with the packed records already
+             in GPU memory (the device-level entry ce_advance_device), timed
+             with CUDA events on the launching stream, max over ranks;
+  e2e     -- the same through the public C ABI with host buffers
+             (ce_submit + ce_poll: upload, kernel, result download);
+  roofline, cpu_baseline, clocks -- see below.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun each rank evaluates its own generation (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "creature-substeps/s at 3M creatures x 20 s"
+UNIT = "creature-substeps/s"
+WORKLOAD = "game"
+WORKLOAD_TEXT = ("3,000,000 seeded synthetic creatures (seed 1), 3-10 nodes, 2-24 muscles, calm flat world, "
+                 "20 s trials at 60 steps/s x 16 substeps, FP32")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--creatures", type=int, default=3_000_000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- workload
+def build_workload(n: int, rank: int):
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS[WORKLOAD]
+    world = w.world()
+    pop = ce.generate(w.spec, n, first=rank * n)
+    wave = ce.pack(pop, world)
+    return world, pop, wave
+
+
+def substeps_run(results: np.ndarray, world) -> float:
+    import evolution_simulator_gpu_b200 as ce
+    rate = world.rate or 60
+    total = ce.trial_steps(world)
+    t = np.where(results["fall_time"] > 0, results["fall_time"] * rate,
+                 np.where(results["screened"] > 0, results["screened"] * rate, total))
+    return float(16.0 * np.minimum(np.round(t), total).sum())
+
+
+def op_counts() -> dict:
+    path = ROOT / "profiles" / "op_counts.json"
+    return json.loads(path.read_text()) if path.exists() else {}
+
+
+def traffic_per_substep():
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    return json.loads(path.read_text()).get(WORKLOAD, {}).get("dram_bytes_per_substep")
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(wave, world, budget_s: float) -> dict:
+    """The CPU oracle (oracle/creature_oracle.cpp, FP32, all host threads) on a
+    bounded sample of the same generation: creatures in packed order from
+    evenly spread chunks until `budget_s` of wall time."""
+    import evolution_simulator_gpu_b200 as ce
+    from oracle.ref import Oracle
+    oracle = Oracle()
+    params = ce.make_params(world)
+    flags = ce.world_flags(world)
+    cores = os.cpu_count() or 1
+    n = len(wave)
+    chunk = 64 * cores
+    starts = np.linspace(0, n - chunk, 64).astype(np.int64)
+    done = secs = 0.0
+    creatures = 0
+    for s in starts:
+        res, t = oracle.run(wave, params, flags, world.rate or 60, int(s), chunk, threads=cores)
+        secs += t
+        done += substeps_run(res, world)
+        creatures += chunk
+        if secs > budget_s:
+            break
+    return {"value": done / secs, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{creatures} creatures of the same generation (chunks spread over the packed order), "
+                      f"{done:.3g} creature-substeps in {secs:.1f} s"}
+
+
+# ---------------------------------------------------------------- engine arm
+def run_engine(args):
+    world_size, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import evolution_simulator_gpu_b200 as ce
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    world, pop, wave = build_workload(args.creatures, rank)
+    eng = ce.Engine(local)
+    flags = ce.world_flags(world)
+    rate = world.rate or 60
+    max_nodes, max_muscles = wave.max_nodes, wave.max_muscles
+    params = ce.make_params(world, 0, len(wave), 0)
+    # Device-resident records (the inputs of the value measurement).
+    d_lanes = torch.from_numpy(wave.lanes.view(np.int32)).to(dev)
+    d_muscles = torch.from_numpy(wave.muscles).to(dev)
+    d_heads = torch.from_numpy(wave.heads.view(np.int32).reshape(-1)).to(dev)
+    d_results = torch.zeros(len(wave) * 19, dtype=torch.float32, device=dev)
+    d_counter = torch.zeros(16, dtype=torch.int32, device=dev)
+    d_scratch = torch.empty(eng.scratch_bytes(flags, rate, max_nodes, max_muscles), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def one_step():
+        d_counter.zero_()
+        eng.advance_device(d_lanes.data_ptr(), d_muscles.data_ptr(), d_heads.data_ptr(), d_results.data_ptr(),
+                           d_counter.data_ptr(), d_scratch.data_ptr(), params, flags, rate, max_nodes, max_muscles,
+                           stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    res = d_results.cpu().numpy().view(ce.RESULT_DTYPE)
+    units = substeps_run(res, world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world_size)
+    torch.cuda.synchronize(dev)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launch_ms = []
+    start.record(stream)
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_step()
+        e1.record(stream)
+        launch_ms.append((e0, e1))
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world_size)
+    clk = clocks.stop()
+    ms = start.elapsed_time(stop)
+    per_launch_ms = float(np.mean([a.elapsed_time(b) for a, b in launch_ms]))
+    ms_max = max_over_ranks(ms, world_size)
+    total_units = sum_over_ranks(units * args.steps, world_size)
+    value = total_units / (ms_max / 1e3)
+
+    # End to end through the C ABI with host buffers.
+    e2e_launches = 0
+    h2d = wave.lanes.nbytes + wave.muscles.nbytes + wave.heads.nbytes + 4 * len(wave)
+    d2h = len(wave) * ce.RESULT_DTYPE.itemsize
+    eng.run(wave, world)  # buffers sized, pinned staging allocated
+    barrier(world_size)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out, busy = eng.run(wave, world)
+        e2e_launches += 1 if wave.max_nodes <= 16 else 2
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, world_size)
+    e2e_value = sum_over_ranks(substeps_run(out, world) * args.steps, world_size) / e2e_s
+    same = bool((out.view(np.uint32) == res.view(np.uint32)).all())
+
+    if rank == 0:
+        counts = op_counts().get(WORKLOAD, {})
+        flops_per = counts.get("flops_per_substep")
+        peak = ce.measure_fp32(local)
+        achieved = flops_per * units / (per_launch_ms / 1e3) / 1e12 if flops_per else None
+        tps = traffic_per_substep()
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak if achieved else None,
+                    "traffic": tps * units if tps else None,
+                    "peak_source": "measured: FP32 multiply-add calibration kernel (ce_measure_fp32) on this GPU",
+                    "numerator": f"{flops_per:.0f} algorithmic FP32 operations per creature-substep "
+                                 "(oracle op count, profiles/op_counts.json) x creature-substeps of the launch"
+                    if flops_per else None}
+        cpu = cpu_baseline(wave, world, args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD_TEXT, "creatures_per_gpu": len(wave),
+                       "trial_steps": ce.trial_steps(world), "substeps_per_step": 16,
+                       "mean_steps_run": units / 16.0 / len(wave),
+                       "l2": "inputs larger than L2 (%.1f GB of packed records per GPU)" % (h2d / 1e9),
+                       "parallelism": f"dp{world_size} (independent generations per GPU)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds_per_step": e2e_s / args.steps, "timing": "host wall clock around ce_submit+ce_poll",
+                    "results_equal_device_path": same},
+            "gpu_launches": args.steps, "gpu_launches_e2e": e2e_launches,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world_size > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference arm: the reference path has no CPU implementation of its
+    own (its only physics is the CUDA kernel, src/physics.rs:3-6), so it is
+    timed as the CPU restatement of that kernel (the oracle port) on all host
+    cores, one bounded sample of the generation per step. The reference's own
+    kernel, built from its source for this GPU, is timed beside it on the same
+    generation (reference_gpu)."""
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import evolution_simulator_gpu_b200 as ce
+    from oracle.ref import Oracle, RefKernel
+    world, pop, wave = build_workload(args.creatures, 0)
+    oracle = Oracle()
+    params = ce.make_params(world)
+    flags = ce.world_flags(world)
+    cores = os.cpu_count() or 1
+    chunk = 32 * cores
+    n = len(wave)
+    rng = np.random.default_rng(0)
+    per_step = max(args.cpu_seconds / 4.0, 2.0)
+
+    def one_step():
+        done = secs = 0.0
+        count = 0
+        while secs < per_step:
+            s = int(rng.integers(0, n - chunk))
+            res, t = oracle.run(wave, params, flags, world.rate or 60, s, chunk, threads=cores)
+            secs += t
+            done += substeps_run(res, world)
+            count += chunk
+        return done, secs, count
+
+    for _ in range(args.warmup):
+        one_step()
+    tot_units = tot_secs = 0.0
+    tot_count = 0
+    for _ in range(args.steps):
+        u, s, c = one_step()
+        tot_units += u
+        tot_secs += s
+        tot_count += c
+    value = tot_units / tot_secs
+    ref_gpu = None
+    try:
+        kern = RefKernel(flags, world.rate or 60)
+        kern.run(wave.take(np.arange(4096)), params)
+        res, ms = kern.run(wave, params)
+        ref_gpu = {"value": substeps_run(res, world) / (ms / 1e3), "unit": UNIT,
+                   "what": "the reference's own kernel (shaders/creature.cu) built for sm_100a with its NVRTC "
+                           "options, launched with its engine's wave and grid rule, CUDA-event time of one "
+                           "generation", "seconds": ms / 1e3}
+    except Exception as exc:  # the reference kernel needs a GPU
+        ref_gpu = {"unavailable": str(exc).splitlines()[0]}
+    sample = f"{tot_count} creatures of the generation in chunks of {chunk}, {tot_units:.3g} creature-substeps"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD_TEXT, "creatures_per_gpu": n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": ref_gpu}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -143,7 +143,8 @@ def _bind(lib: C.CDLL) -> None:
         "ce_pack": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_frame_stride": (C.c_uint32, [C.c_uint32]),
-        "ce_generate_size": (C.c_int, [P(GenSpec), C.c_size_t, P(C.c_size_t), P(C.c_size_t), P(C.c_size_t)]),
+        "ce_generate_size": (C.c_int, [P(GenSpec), C.c_size_t, C.c_size_t, P(C.c_size_t), P(C.c_size_t),
+                                       P(C.c_size_t)]),
         "ce_generate": (C.c_int, [P(GenSpec), C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p]),
         "ce_to_metrics": (C.c_int, [C.c_void_p, C.c_uint32, P(World), C.c_void_p]),
@@ -164,6 +165,9 @@ def _bind(lib: C.CDLL) -> None:
                                         C.c_void_p, P(Params), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p]),
         "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
+        "ce_measure_fp32": (C.c_int, [C.c_int, P(C.c_double), P(C.c_double)]),
+        "ce_to_metrics_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
+        "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -185,7 +189,8 @@ def lib() -> C.CDLL:
 EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_frame_stride", "ce_generate_size",
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
-            "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault"]
+            "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
+            "ce_to_metrics_batch", "ce_niche_batch"]
 
 
 def _check(status: int, what: str) -> None:
@@ -324,24 +329,15 @@ def generate(spec: GenSpecPy, count: int, first: int = 0) -> Population:
     L = lib()
     cs = spec.c()
     nn, nb, nm = C.c_size_t(), C.c_size_t(), C.c_size_t()
-    if first == 0:
-        _check(L.ce_generate_size(C.byref(cs), count, C.byref(nn), C.byref(nb), C.byref(nm)), "ce_generate_size")
-        sizes = (nn.value, nb.value, nm.value)
-    else:
-        sizes = (count * MAX_NODES, count * MAX_NODES, count * MAX_MUSCLES)
-    nodes = np.zeros(sizes[0], NODE_DTYPE)
-    bones = np.zeros(sizes[1], BONE_DTYPE)
-    muscles = np.zeros(sizes[2], MUSCLE_DTYPE)
-    strength = np.zeros(sizes[2], np.float32)
+    _check(L.ce_generate_size(C.byref(cs), first, count, C.byref(nn), C.byref(nb), C.byref(nm)),
+           "ce_generate_size")
+    nodes = np.zeros(nn.value, NODE_DTYPE)
+    bones = np.zeros(nb.value, BONE_DTYPE)
+    muscles = np.zeros(nm.value, MUSCLE_DTYPE)
+    strength = np.zeros(nm.value, np.float32)
     genomes = np.zeros(count, GENOME_DTYPE)
     _check(L.ce_generate(C.byref(cs), first, count, _ptr(nodes), _ptr(bones), _ptr(muscles), _ptr(strength),
                          _ptr(genomes)), "ce_generate")
-    if first != 0 and count:
-        last = genomes[-1]
-        nodes = nodes[:last["node_start"] + last["node_count"]].copy()
-        bones = bones[:last["bone_start"] + last["bone_count"]].copy()
-        muscles = muscles[:last["muscle_start"] + last["muscle_count"]].copy()
-        strength = strength[:last["muscle_start"] + last["muscle_count"]].copy()
     return Population(nodes, bones, muscles, genomes, strength)
 
 
@@ -545,13 +541,33 @@ def evaluate(engine: Engine, pop: Population, world: World, indices=None) -> np.
 
 # ---------------------------------------------------------------- metrics
 def to_metrics(results: np.ndarray, node_counts: np.ndarray, world: World) -> np.ndarray:
+    """scheduler::to_metrics for every result (src/scheduler.rs:890-923)."""
     out = np.zeros(len(results), METRICS_DTYPE)
-    L = lib()
-    res = np.ascontiguousarray(results)
-    for i in range(len(results)):
-        _check(L.ce_to_metrics(res[i:i + 1].ctypes.data, int(node_counts[i]), C.byref(world),
-                               out[i:i + 1].ctypes.data), "ce_to_metrics")
+    res = np.ascontiguousarray(results, RESULT_DTYPE)
+    nc = np.ascontiguousarray(node_counts, np.uint32)
+    _check(lib().ce_to_metrics_batch(res.ctypes.data, nc.ctypes.data, len(res), C.byref(world), out.ctypes.data),
+           "ce_to_metrics_batch")
     return out
+
+
+def niche_cells(pop: Population, metrics: np.ndarray, indices=None, global_layout: bool = True) -> np.ndarray:
+    """Dense niche cells (src/qd.rs:762-846, 988-999) of creatures `indices`
+    (default: all, in order) with their metrics rows."""
+    n = len(metrics)
+    idx = None if indices is None else np.ascontiguousarray(indices, np.uint32)
+    m = np.ascontiguousarray(metrics, METRICS_DTYPE)
+    cells = np.zeros(n, np.int64)
+    pc = pop.c()
+    _check(lib().ce_niche_batch(C.byref(pc), _ptr(idx), n, m.ctypes.data, 1 if global_layout else 0,
+                                cells.ctypes.data), "ce_niche_batch")
+    return cells
+
+
+def measure_fp32(device: int = 0) -> float:
+    """The FP32 multiply-add rate of the GPU in TFLOP/s (calibration kernel)."""
+    t, s = C.c_double(), C.c_double()
+    _check(lib().ce_measure_fp32(device, C.byref(t), C.byref(s)), "ce_measure_fp32")
+    return t.value
 
 
 def niche(pop: Population, i: int, metrics_row: np.ndarray, global_layout: bool = True):

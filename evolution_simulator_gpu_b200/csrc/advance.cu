@@ -13,7 +13,18 @@ namespace cek {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-template <class W, int NS, bool RECORD, int RATE>
+// The ground under a node for the step's contact tallies, as a call rather
+// than inlined: the reference kernel's tallies compute the ground through a
+// call too, and only with the same call boundary do the contact tests round
+// the same (an inlined ground lets the compiler fuse the floor height's
+// multiply-add with the ground's last term, which moves a contact test at
+// its edge by one unit in the last place).
+template <class W>
+__device__ __noinline__ float2 ground_call(const W& w, float x, float amp, float qphase, const ce_params& p) {
+    return ground(w, x, amp, qphase, p);
+}
+
+template <class W, bool RECORD, int RATE>
 struct Trial {
     using C = Clock<RATE>;
     using Body = Creature<W, RATE, RECORD>;
@@ -30,7 +41,7 @@ struct Trial {
         }
         for (unsigned k = 0u; k < b.r.muscles; k++) {
             fr[CE_MAX_NODES + k] =
-                make_float2(b.L.word(b.S.muscle + 5u * k + kMState, 0), b.L.word(b.S.rec_pull + k / 4u, k % 4u));
+                make_float2(b.t.muscle(k).x, b.L.word(b.S.rec_pull + k / 4u, k % 4u));
         }
         const unsigned long long broken = b.broken_joints();
         fr[stride - 1u] =
@@ -108,7 +119,8 @@ struct Trial {
             L.put(m0 + kPull1, __ldg(q + 1));
             L.put(m0 + kRhythm0, __ldg(q + 2));
             L.put(m0 + kRhythm1, __ldg(q + 3));
-            L.put(m0 + kMState, make_float4(1.0f, 0.0f, 0.0f, __ldg(q + 4).x));
+            L.put(m0 + kMState, make_float4(0.0f, 0.0f, 0.0f, __ldg(q + 4).x));
+            b.t.muscle(k) = make_float2(1.0f, 0.0f);
             if (RECORD) {
                 L.word(S.rec_pull + k / 4u, k % 4u) = 0.0f;
             }
@@ -175,7 +187,7 @@ struct Trial {
             low = fminf(low, q.y - nr.z);
             high = fmaxf(high, q.y + nr.z);
             if (b.w.has(CE_FLAG_GROUND)) {
-                const float2 g = ground(b.w, q.x, r.amp, r.qphase, p);
+                const float2 g = ground_call(b.w, q.x, r.amp, r.qphase, p);
                 const float floor_y = g.x + nr.z * sqrtf(1.0f + g.y * g.y);
                 if (q.y <= floor_y + kContactSlack) {
                     touching |= 1u << i;
@@ -313,7 +325,7 @@ struct Trial {
                 const float touched = (float)__popc(contact_bits) / (float)r.nodes;
                 float en_mean = 0.0f;
                 for (unsigned k = 0u; k < r.muscles; k++) {
-                    en_mean += L.word(S.muscle + 5u * k + kMState, 0);
+                    en_mean += b.t.muscle(k).x;
                 }
                 en_mean /= (float)max(r.muscles, 1u);
                 contact_hi = __uint_as_float((__float_as_uint(contact_hi) & keep) | (f2h(com_x) << sh));
@@ -448,15 +460,16 @@ struct Trial {
     }
 };
 
-template <class W, int NS, bool RECORD, int RATE>
+template <class W, bool RECORD, int RATE>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const KernelArgs a, const ce_params p,
                                                                       const W w) {
     extern __shared__ float4 smem[];
-    using T = Trial<W, NS, RECORD, RATE>;
+    using T = Trial<W, RECORD, RATE>;
     const unsigned threads = blockDim.x;
-    const NodeTables tab{smem + threadIdx.x, reinterpret_cast<float2*>(smem + NS * threads) + threadIdx.x,
+    float2* fp_base = reinterpret_cast<float2*>(smem + a.rows * threads);
+    const NodeTables tab{smem + threadIdx.x, fp_base + threadIdx.x, fp_base + a.rows * threads + threadIdx.x,
                          threads};
-    const SlotLayout S = SlotLayout::make(NS, a.mm, RECORD);
+    const SlotLayout S = SlotLayout::make(a.rows, a.mm, RECORD);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = (blockIdx.x * threads + threadIdx.x) >> 5u;
     const unsigned warps_total = gridDim.x * (threads >> 5u);
@@ -514,34 +527,43 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const Kerne
     }
 }
 
-template <class W, int NS, bool RECORD, int RATE>
+// Shared memory carveout (percent of the largest) that fits `blocks`
+// blocks of `smem` bytes each, leaving the rest of the multiprocessor's
+// memory to the L1 cache that holds the creatures' constant lines.
+static int carveout_for(size_t smem, int blocks) {
+    const size_t need = (smem + 1024u) * (size_t)blocks;
+    const size_t full = 228u * 1024u;
+    int pct = (int)((need * 100u + full - 1u) / full);
+    return pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+}
+
+template <class W, bool RECORD, int RATE>
+static cudaError_t occupancy_one(unsigned rows, unsigned mm, unsigned block, int* blocks) {
+    auto kern = advance_kernel<W, RECORD, RATE>;
+    const size_t smem = smem_bytes(rows, mm, block);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kern, (int)block, smem);
+}
+
+template <class W, bool RECORD, int RATE>
 static cudaError_t launch_one(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const W& w) {
-    auto kern = advance_kernel<W, NS, RECORD, RATE>;
-    const size_t smem = smem_bytes(NS, s.block);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(NS, 256));
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    auto kern = advance_kernel<W, RECORD, RATE>;
+    const size_t smem = smem_bytes(s.rows, s.mm, s.block);
+    int blocks = 0;
+    cudaError_t e = occupancy_one<W, RECORD, RATE>(s.rows, s.mm, s.block, &blocks);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             carveout_for(smem, blocks > 0 ? blocks : 1));
+    if (e != cudaSuccess) return e;
     kern<<<s.grid, s.block, smem, s.stream>>>(a, p, w);
     return cudaGetLastError();
 }
 
-template <class W, int NS, bool RECORD, int RATE>
-static cudaError_t occupancy_one(unsigned block, int* blocks) {
-    auto kern = advance_kernel<W, NS, RECORD, RATE>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(NS, 256));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kern, (int)block, smem_bytes(NS, block));
-}
-
 // The compiled worlds. Any other world runs on the run-time-world kernel.
-template <int NS, bool RECORD, int RATE, class F>
+template <bool RECORD, int RATE, class F>
 static cudaError_t by_world(uint32_t flags, F&& f) {
     switch (flags) {
         case kWorldCalm: return f(StaticWorld<kWorldCalm>{});
@@ -552,57 +574,42 @@ static cudaError_t by_world(uint32_t flags, F&& f) {
     }
 }
 
-template <int NS, bool RECORD, int RATE>
-static cudaError_t dispatch_world(const LaunchSpec& s, const KernelArgs& a, const ce_params& p) {
-    return by_world<NS, RECORD, RATE>(s.flags, [&](auto w) { return launch_one<decltype(w), NS, RECORD, RATE>(s, a, p, w); });
-}
-template <int NS, bool RECORD, int RATE>
-static cudaError_t occupancy_world(uint32_t flags, unsigned block, int* blocks) {
-    return by_world<NS, RECORD, RATE>(flags, [&](auto w) { return occupancy_one<decltype(w), NS, RECORD, RATE>(block, blocks); });
-}
-
 template <bool RECORD, int RATE>
-static cudaError_t dispatch_ns(const LaunchSpec& s, const KernelArgs& a, const ce_params& p) {
-    switch (s.ns) {
-        case 8: return dispatch_world<8, RECORD, RATE>(s, a, p);
-        case 16: return dispatch_world<16, RECORD, RATE>(s, a, p);
-        case 32: return dispatch_world<32, RECORD, RATE>(s, a, p);
-        default: return cudaErrorInvalidValue;
-    }
+static cudaError_t dispatch(const LaunchSpec& s, const KernelArgs& a, const ce_params& p) {
+    return by_world<RECORD, RATE>(s.flags, [&](auto w) { return launch_one<decltype(w), RECORD, RATE>(s, a, p, w); });
 }
 
 cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p) {
+    if (s.rows < 2 || s.rows > CE_MAX_NODES || s.mm > CE_MAX_MUSCLES || a.rows != s.rows || a.mm != s.mm) {
+        return cudaErrorInvalidValue;
+    }
     if (s.rate == 60) {
-        return s.record ? dispatch_ns<true, 60>(s, a, p) : dispatch_ns<false, 60>(s, a, p);
+        return s.record ? dispatch<true, 60>(s, a, p) : dispatch<false, 60>(s, a, p);
     }
     if (s.rate == 120) {
-        return s.record ? dispatch_ns<true, 120>(s, a, p) : dispatch_ns<false, 120>(s, a, p);
+        return s.record ? dispatch<true, 120>(s, a, p) : dispatch<false, 120>(s, a, p);
     }
     return cudaErrorInvalidValue;
 }
 
-cudaError_t advance_occupancy(unsigned ns, uint32_t flags, bool record, int rate, unsigned block, int* blocks) {
+cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block,
+                              int* blocks) {
     auto go = [&](auto rec_tag, auto rate_tag) -> cudaError_t {
         constexpr bool R = decltype(rec_tag)::value;
         constexpr int RT = decltype(rate_tag)::value;
-        switch (ns) {
-            case 8: return occupancy_world<8, R, RT>(flags, block, blocks);
-            case 16: return occupancy_world<16, R, RT>(flags, block, blocks);
-            case 32: return occupancy_world<32, R, RT>(flags, block, blocks);
-            default: return cudaErrorInvalidValue;
-        }
+        return by_world<R, RT>(flags, [&](auto w) { return occupancy_one<decltype(w), R, RT>(rows, mm, block, blocks); });
     };
-    using T = std::true_type;
-    using F = std::false_type;
+    using Tt = std::true_type;
+    using Ft = std::false_type;
     using R60 = std::integral_constant<int, 60>;
     using R120 = std::integral_constant<int, 120>;
-    if (rate == 60) return record ? go(T{}, R60{}) : go(F{}, R60{});
-    if (rate == 120) return record ? go(T{}, R120{}) : go(F{}, R120{});
+    if (rate == 60) return record ? go(Tt{}, R60{}) : go(Ft{}, R60{});
+    if (rate == 120) return record ? go(Tt{}, R120{}) : go(Ft{}, R120{});
     return cudaErrorInvalidValue;
 }
 
 }  // namespace cek
 
 namespace cek {
-unsigned slot_lines(unsigned ns, unsigned mm, bool record) { return SlotLayout::make(ns, mm, record).lines; }
+unsigned slot_lines(unsigned rows, unsigned mm, bool record) { return SlotLayout::make(rows, mm, record).lines; }
 }  // namespace cek

@@ -102,7 +102,7 @@ struct Creature {
         for (unsigned k = 0u; k < r.muscles; k++) {
             const unsigned m0 = S.muscle + 5u * k;
             const float4 r0 = L.get(m0 + kRhythm0), r1 = L.get(m0 + kRhythm1);
-            float& demand = L.word(m0 + kMState, 1);
+            float& demand = t.muscle(k).y;
             const float offset = L.word(m0 + kMState, 2);
             const float before = rhythm(t_now, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
             const float after = rhythm(t_now + C::dt, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
@@ -121,7 +121,7 @@ struct Creature {
         for (unsigned k = 0u; k < r.muscles; k++) {
             const unsigned m0 = S.muscle + 5u * k;
             const float4 q0 = L.get(m0 + kPull0), q1 = L.get(m0 + kPull1);
-            const float2 ms = *reinterpret_cast<const float2*>(&L.word(m0 + kMState, 0));
+            const float2 ms = t.muscle(k);
             const unsigned nodes = __float_as_uint(q0.x);
             const unsigned a0 = nodes & 255u, a1 = (nodes >> 8u) & 255u, b0 = (nodes >> 16u) & 255u,
                            b1 = nodes >> 24u;
@@ -146,7 +146,7 @@ struct Creature {
             }
             const float active = clampf(drive + lengthening * 0.15f, -cap, cap);
             const float work = fminf(drive, cap) * fmaxf(-lengthening, 0.0f) * C::h;
-            L.word(m0 + kMState, 0) = clampf(ms.x - work * inv_capacity * p.inv_muscle_energy +
+            t.muscle(k).x = clampf(ms.x - work * inv_capacity * p.inv_muscle_energy +
                                                  kMuscleRecovery * p.muscle_recovery * C::h * (1.0f - ms.x),
                                              0.0f, 1.0f);
             const float tendon = tendon_k * fmaxf(len - slack, 0.0f);

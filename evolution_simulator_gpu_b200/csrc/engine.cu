@@ -2,9 +2,10 @@
 // each with its stream, events, pinned staging and device buffers.
 //
 // A submission (the reference's CudaEngine::launch, src/cuda_engine.rs:
-// 2106-2316) uploads the packed batch, splits it into size classes by node
-// count (8, 16 or 32 node rows a lane), runs one persistent launch per class,
-// and reads the results back, all on the slot's stream. ce_poll hands back
+// 2106-2316) uploads the packed batch, splits it into two size classes by
+// node count (bodies of at most 16 nodes, and larger ones), runs one
+// persistent launch per class, the two side by side on two streams so that
+// the tail of one overlaps the other, and reads the results back. ce_poll hands back
 // the oldest finished submission with its GPU-busy seconds, as the
 // reference's poll does (src/cuda_engine.rs:2319-2393).
 #include <cuda_runtime.h>
@@ -26,7 +27,8 @@ using ce::set_error;
 
 namespace {
 
-constexpr unsigned kClasses[3] = {8u, 16u, 32u};
+// Bodies of up to this many nodes form the first size class.
+constexpr unsigned kSmallBody = 16u;
 
 ce_status cuda_status(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return CE_OK;
@@ -84,8 +86,8 @@ struct PinnedBuf {
 };
 
 struct ClassPlan {
-    unsigned ns;
     uint32_t first, count;  // range of the order list
+    uint32_t rows;          // most nodes in the class
     uint32_t mm;            // most muscles in the class
 };
 
@@ -93,8 +95,8 @@ struct Slot {
     bool busy = false;
     uint64_t ticket = 0;
     size_t count = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t start = nullptr, stop = nullptr, done = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr;  // side: the second class
+    cudaEvent_t start = nullptr, stop = nullptr, done = nullptr, joined = nullptr;
     DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_order, d_counters, d_scratch;
     PinnedBuf h_upload, h_results;
     std::chrono::steady_clock::time_point submitted;
@@ -121,11 +123,12 @@ namespace {
 ce_status set_device(ce_engine* e) { return cuda_status(cudaSetDevice(e->device), "cudaSetDevice"); }
 
 // The grid of a persistent launch for a class: every block that fits.
-unsigned grid_for(ce_engine* e, unsigned ns, uint32_t flags, bool record, int rate, size_t count) {
+unsigned grid_for(ce_engine* e, unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, size_t count) {
     int per_sm = 0;
     if (e->ctas_per_sm) {
         per_sm = (int)e->ctas_per_sm;
-    } else if (cek::advance_occupancy(ns, flags, record, rate, cek::kBlock, &per_sm) != cudaSuccess || per_sm < 1) {
+    } else if (cek::advance_occupancy(rows, mm, flags, record, rate, cek::kBlock, &per_sm) != cudaSuccess ||
+               per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;
     }
@@ -134,12 +137,10 @@ unsigned grid_for(ce_engine* e, unsigned ns, uint32_t flags, bool record, int ra
     return (unsigned)std::max<size_t>(1, std::min(needed, full));
 }
 
-size_t scratch_bytes(unsigned grid, unsigned ns, unsigned mm, bool record) {
+size_t scratch_bytes(unsigned grid, unsigned rows, unsigned mm, bool record) {
     const size_t warps = (size_t)grid * (cek::kBlock / 32u);
-    return warps * cek::slot_lines(ns, mm, record) * 32u * 16u;
+    return warps * cek::slot_lines(rows, mm, record) * 32u * 16u;
 }
-
-unsigned class_of_nodes(unsigned n) { return n <= 8 ? 8u : (n <= 16 ? 16u : 32u); }
 
 ce_status check_world(const ce_world* w) {
     if (!w) {
@@ -164,8 +165,8 @@ ce_status plan_classes(const ce_wave_pack* pack, std::vector<uint32_t>& order, s
     order.clear();
     plans.clear();
     order.reserve(pack->count);
-    for (unsigned ns : kClasses) {
-        ClassPlan c{ns, (uint32_t)order.size(), 0, 0};
+    for (int big = 0; big < 2; big++) {
+        ClassPlan c{(uint32_t)order.size(), 0, 2, 0};
         for (size_t i = 0; i < pack->count; i++) {
             const uint32_t* h = pack->heads + 8 * i;
             const unsigned n = h[0] & 255u, m = h[1];
@@ -174,8 +175,9 @@ ce_status plan_classes(const ce_wave_pack* pack, std::vector<uint32_t>& order, s
                           std::to_string(m) + " muscles");
                 return CE_ERR_INVALID;
             }
-            if (class_of_nodes(n) != ns) continue;
+            if ((n > kSmallBody) != (big != 0)) continue;
             order.push_back((uint32_t)i);
+            c.rows = std::max(c.rows, n);
             c.mm = std::max(c.mm, m);
         }
         c.count = (uint32_t)order.size() - c.first;
@@ -222,6 +224,9 @@ extern "C" ce_status ce_open(int device, const ce_options* options, ce_engine** 
     e->slots.resize(nslots);
     for (Slot& sl : e->slots) {
         s = cuda_status(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (s == CE_OK) s = cuda_status(cudaStreamCreateWithFlags(&sl.side, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (s == CE_OK)
+            s = cuda_status(cudaEventCreateWithFlags(&sl.joined, cudaEventDisableTiming), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.start), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.stop), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "cudaEventCreate");
@@ -251,6 +256,8 @@ extern "C" ce_status ce_close(ce_engine* e) {
         if (sl.start) cudaEventDestroy(sl.start);
         if (sl.stop) cudaEventDestroy(sl.stop);
         if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.joined) cudaEventDestroy(sl.joined);
+        if (sl.side) cudaStreamDestroy(sl.side);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     e->rec_frames.release();
@@ -340,13 +347,15 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     const int rate = (int)ce::world_rate(*w);
     ce_params p;
     ce_make_params(w, 0, (uint32_t)pack->count, 0, &p);
-    // Grids and scratch of the classes, which run one after another on the
-    // slot's stream and share its scratch.
+    // Grids and scratch of the classes, which run side by side, each with its
+    // own part of the slot's scratch.
     std::vector<unsigned> grids(plans.size());
+    std::vector<size_t> scratch_at(plans.size());
     size_t scratch = 0;
     for (size_t c = 0; c < plans.size(); c++) {
-        grids[c] = grid_for(e, plans[c].ns, flags, false, rate, plans[c].count);
-        scratch = std::max(scratch, scratch_bytes(grids[c], plans[c].ns, plans[c].mm, false));
+        grids[c] = grid_for(e, plans[c].rows, plans[c].mm, flags, false, rate, plans[c].count);
+        scratch_at[c] = scratch;
+        scratch += (scratch_bytes(grids[c], plans[c].rows, plans[c].mm, false) + 255u) & ~(size_t)255u;
     }
     const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
     const size_t order_b = order.size() * 4, res_b = pack->count * sizeof(ce_result);
@@ -373,6 +382,7 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     }
     CE_TRY(cudaMemsetAsync(sl.d_counters.ptr, 0, 64, st), "cudaMemsetAsync");
     CE_TRY(cudaEventRecord(sl.start, st), "cudaEventRecord");
+    CE_TRY(cudaStreamWaitEvent(sl.side, sl.start, 0), "cudaStreamWaitEvent");
     for (size_t c = 0; c < plans.size(); c++) {
         cek::KernelArgs a{};
         a.records = static_cast<const uint32_t*>(sl.d_lanes.ptr);
@@ -380,16 +390,20 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
         a.heads = static_cast<const uint4*>(sl.d_heads.ptr);
         a.results = static_cast<ce_result*>(sl.d_results.ptr);
         a.counter = static_cast<uint32_t*>(sl.d_counters.ptr) + c;
-        a.scratch = static_cast<float4*>(sl.d_scratch.ptr);
+        a.scratch = reinterpret_cast<float4*>(static_cast<char*>(sl.d_scratch.ptr) + scratch_at[c]);
         a.frames = nullptr;
         a.order = static_cast<const uint32_t*>(sl.d_order.ptr) + plans[c].first;
         a.count = plans[c].count;
+        a.rows = plans[c].rows;
         a.mm = plans[c].mm;
         a.frames_per_creature = 0;
         a.chunk_k = e->chunk_k;
-        cek::LaunchSpec ls{plans[c].ns, flags, false, rate, grids[c], cek::kBlock, st};
+        cek::LaunchSpec ls{plans[c].rows, plans[c].mm, flags, false, rate, grids[c], cek::kBlock,
+                           c == 0 ? st : sl.side};
         CE_TRY(cek::launch_advance(ls, a, p), "advance launch");
     }
+    CE_TRY(cudaEventRecord(sl.joined, sl.side), "cudaEventRecord");
+    CE_TRY(cudaStreamWaitEvent(st, sl.joined, 0), "cudaStreamWaitEvent");
     CE_TRY(cudaEventRecord(sl.stop, st), "cudaEventRecord");
     CE_TRY(cudaMemcpyAsync(sl.h_results.ptr, sl.d_results.ptr, res_b, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     CE_TRY(cudaEventRecord(sl.done, st), "cudaEventRecord");
@@ -473,9 +487,9 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     std::vector<uint32_t> order;
     std::vector<ClassPlan> plans;
     if ((s = plan_classes(pack, order, plans)) != CE_OK) return s;
-    unsigned ns = 8, mm = 0;
+    unsigned rows = 2, mm = 0;
     for (const ClassPlan& c : plans) {
-        ns = std::max(ns, c.ns);
+        rows = std::max(rows, c.rows);
         mm = std::max(mm, c.mm);
     }
     const uint32_t flags = ce_world_flags(w);
@@ -495,7 +509,7 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     const size_t res_b = pack->count * sizeof(ce_result);
     if ((s = e->rec_frames.ensure(frame_floats * 4)) || (s = e->rec_lanes.ensure(lanes_b)) ||
         (s = e->rec_muscles.ensure(mus_b)) || (s = e->rec_heads.ensure(heads_b)) || (s = e->rec_results.ensure(res_b)) ||
-        (s = e->rec_counter.ensure(4)) || (s = e->rec_scratch.ensure(scratch_bytes(grid, ns, mm, true)))) {
+        (s = e->rec_counter.ensure(4)) || (s = e->rec_scratch.ensure(scratch_bytes(grid, rows, mm, true)))) {
         return s;
     }
     CE_TRY(cudaMemcpy(e->rec_lanes.ptr, pack->lanes, lanes_b, cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -513,10 +527,11 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     a.frames = static_cast<float2*>(e->rec_frames.ptr);
     a.order = nullptr;
     a.count = (uint32_t)pack->count;
+    a.rows = rows;
     a.mm = mm;
     a.frames_per_creature = per;
     a.chunk_k = 1;
-    cek::LaunchSpec ls{ns, flags, true, rate, grid, cek::kBlock, nullptr};
+    cek::LaunchSpec ls{rows, mm, flags, true, rate, grid, cek::kBlock, nullptr};
     CE_TRY(cek::launch_advance(ls, a, p), "record launch");
     CE_TRY(cudaDeviceSynchronize(), "record kernel");
     CE_TRY(cudaMemcpy(frames, e->rec_frames.ptr, frame_floats * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
@@ -528,9 +543,8 @@ extern "C" size_t ce_advance_scratch_bytes(ce_engine* e, uint32_t world_flags, u
                                            uint32_t max_muscles) {
     if (!e || max_nodes < 2 || max_nodes > CE_MAX_NODES || max_muscles > CE_MAX_MUSCLES) return 0;
     if (rate != 60 && rate != 120) return 0;
-    const unsigned ns = class_of_nodes(max_nodes);
-    const unsigned grid = grid_for(e, ns, world_flags, false, (int)rate, (size_t)1 << 30);
-    return scratch_bytes(grid, ns, max_muscles, false);
+    const unsigned grid = grid_for(e, max_nodes, max_muscles, world_flags, false, (int)rate, (size_t)1 << 30);
+    return scratch_bytes(grid, max_nodes, max_muscles, false);
 }
 
 extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, const float* muscles,
@@ -547,8 +561,7 @@ extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, co
         return CE_ERR_INVALID;
     }
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
-    const unsigned ns = class_of_nodes(max_nodes);
-    const unsigned grid = grid_for(e, ns, world_flags, false, (int)rate, params->count);
+    const unsigned grid = grid_for(e, max_nodes, max_muscles, world_flags, false, (int)rate, params->count);
     cek::KernelArgs a{};
     a.records = records;
     a.muscles = muscles;
@@ -559,10 +572,12 @@ extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, co
     a.frames = nullptr;
     a.order = nullptr;
     a.count = params->count;
+    a.rows = max_nodes;
     a.mm = max_muscles;
     a.frames_per_creature = 0;
     a.chunk_k = e->chunk_k;
-    cek::LaunchSpec ls{ns, world_flags, false, (int)rate, grid, cek::kBlock, static_cast<cudaStream_t>(stream)};
+    cek::LaunchSpec ls{max_nodes, max_muscles, world_flags, false, (int)rate, grid, cek::kBlock,
+                       static_cast<cudaStream_t>(stream)};
     CE_TRY(cek::launch_advance(ls, a, *params), "advance launch");
     return CE_OK;
 }

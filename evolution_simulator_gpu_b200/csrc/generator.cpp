@@ -198,8 +198,8 @@ Body make_body(const ce_gen_spec& s, uint64_t index) {
 
 }  // namespace
 
-extern "C" ce_status ce_generate_size(const ce_gen_spec* spec, size_t count, size_t* nodes, size_t* bones,
-                                      size_t* muscles) {
+extern "C" ce_status ce_generate_size(const ce_gen_spec* spec, size_t first, size_t count, size_t* nodes,
+                                      size_t* bones, size_t* muscles) {
     if (!spec || !nodes || !bones || !muscles) {
         ce::set_error("ce_generate_size: null argument");
         return CE_ERR_INVALID;
@@ -207,7 +207,7 @@ extern "C" ce_status ce_generate_size(const ce_gen_spec* spec, size_t count, siz
     size_t nn = 0, nb = 0, nm = 0;
 #pragma omp parallel for reduction(+ : nn, nb, nm) schedule(dynamic, 1024)
     for (long long i = 0; i < (long long)count; i++) {
-        const Body b = make_body(*spec, (uint64_t)i);
+        const Body b = make_body(*spec, first + (uint64_t)i);
         nn += b.nodes.size();
         nb += b.bones.size();
         nm += b.muscles.size();

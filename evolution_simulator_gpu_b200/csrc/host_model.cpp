@@ -871,3 +871,31 @@ extern "C" int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint
     }
     return index;
 }
+
+extern "C" ce_status ce_to_metrics_batch(const ce_result* r, const uint32_t* node_counts, size_t n,
+                                         const ce_world* w, ce_metrics* out) {
+    if (!r || !node_counts || !w || !out) {
+        set_error("ce_to_metrics_batch: null argument");
+        return CE_ERR_INVALID;
+    }
+    for (size_t i = 0; i < n; i++) {
+        const ce_status s = ce_to_metrics(r + i, node_counts[i], w, out + i);
+        if (s != CE_OK) return s;
+    }
+    return CE_OK;
+}
+
+extern "C" ce_status ce_niche_batch(const ce_population* pop, const uint32_t* indices, size_t n,
+                                    const ce_metrics* m, int global_layout, int64_t* cells) {
+    if (!pop || !m || !cells) {
+        set_error("ce_niche_batch: null argument");
+        return CE_ERR_INVALID;
+    }
+#pragma omp parallel for schedule(static, 4096)
+    for (long long k = 0; k < (long long)n; k++) {
+        const size_t i = indices ? indices[k] : (size_t)k;
+        const ce_genome& g = pop->genomes[i];
+        cells[k] = ce_niche(pop->nodes + g.node_start, g.node_count, g.muscle_count, m + k, global_layout, nullptr);
+    }
+    return CE_OK;
+}

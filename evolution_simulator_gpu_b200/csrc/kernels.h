@@ -25,8 +25,11 @@ constexpr uint32_t kWorldEffectsQuake = kWorldEffects | CE_FLAG_QUAKE;
 constexpr uint32_t kWorldAll = 0xfffu;
 
 // Shared memory of a block: the position/velocity table (16 bytes) and the
-// force table (8 bytes) for `ns` node rows of every thread.
-inline size_t smem_bytes(unsigned ns, unsigned block) { return (size_t)ns * block * 24u; }
+// force table (8 bytes) for `rows` node rows of every thread, and the
+// (energy store, demand) pair of `mm` muscles of every thread.
+inline size_t smem_bytes(unsigned rows, unsigned mm, unsigned block) {
+    return (size_t)block * (rows * 24u + (mm > 0 ? mm : 1u) * 8u);
+}
 
 struct KernelArgs {
     const uint32_t* records;
@@ -38,13 +41,15 @@ struct KernelArgs {
     float2* frames;                // RECORD: frames of each recorded creature
     const uint32_t* order;         // packed positions of this launch's creatures
     uint32_t count;                // creatures of this launch
+    uint32_t rows;                 // node rows: most nodes of a body of this launch
     uint32_t mm;                   // most muscles of a body of this launch
     uint32_t frames_per_creature;  // RECORD: frames of one recording
     uint32_t chunk_k;              // claims shrink to 1 / chunk_k of the rest per warp
 };
 
 struct LaunchSpec {
-    unsigned ns;     // node rows: 8, 16 or 32
+    unsigned rows;   // node rows of the tables (most nodes of a body)
+    unsigned mm;     // most muscles of a body
     uint32_t flags;  // world effect bits
     bool record;
     int rate;        // steps per second: 60 or 120
@@ -52,10 +57,11 @@ struct LaunchSpec {
     cudaStream_t stream;
 };
 
-// 16-byte lines of one lane's slot for a class.
-unsigned slot_lines(unsigned ns, unsigned mm, bool record);
+// 16-byte lines of one lane's slot.
+unsigned slot_lines(unsigned rows, unsigned mm, bool record);
 
 cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
-cudaError_t advance_occupancy(unsigned ns, uint32_t flags, bool record, int rate, unsigned block, int* blocks);
+cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block,
+                              int* blocks);
 
 }  // namespace cek

@@ -165,6 +165,7 @@ __device__ __forceinline__ float ice_at(float x) {
 struct NodeTables {
     float4* pv;  // (x, y, vx, vy)
     float2* fp;  // muscle force, then the position at the start of the substep
+    float2* ms;  // per muscle: (energy store, demand of the step)
     unsigned stride;  // threads of the block
     __device__ __forceinline__ float4& at(unsigned i) const { return pv[i * stride]; }
     __device__ __forceinline__ float2& f(unsigned i) const { return fp[i * stride]; }
@@ -174,6 +175,7 @@ struct NodeTables {
     __device__ __forceinline__ float2& vel(unsigned i) const {
         return *reinterpret_cast<float2*>(&pv[i * stride].z);
     }
+    __device__ __forceinline__ float2& muscle(unsigned k) const { return ms[k * stride]; }
 };
 
 // The 16-byte constant lines of a lane's creature.
@@ -210,8 +212,9 @@ struct SlotLayout {
 constexpr unsigned kWContact = 19, kWLift = 20, kWGround = 21, kWHeadShake = 22, kWHeadAt = 23,
                    kWHeadVel = 25, kWRungX = 27, kWRungSpeed = 28, kWRungEarly = 29, kWRungLate = 30,
                    kWRungBits = 31;
-// Lines of muscle k: pull 0 and 1, rhythm 0 and 1, and its state
-// (energy store, demand, touchdown offset, sensor).
+// Lines of muscle k: pull 0 and 1, rhythm 0 and 1, and its state line
+// (unused, unused, touchdown offset, sensor); the energy store and the
+// step's demand live in shared memory (NodeTables::muscle).
 constexpr unsigned kPull0 = 0, kPull1 = 1, kRhythm0 = 2, kRhythm1 = 3, kMState = 4;
 
 }  // namespace cek

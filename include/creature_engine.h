@@ -211,9 +211,10 @@ typedef struct ce_gen_spec {
     uint64_t first_id;
 } ce_gen_spec;
 
-/* Counts of the genes that ce_generate writes for `count` creatures. */
-ce_status ce_generate_size(const ce_gen_spec* spec, size_t count, size_t* nodes, size_t* bones,
-                           size_t* muscles);
+/* Counts of the genes that ce_generate writes for creatures
+ * [first, first + count). */
+ce_status ce_generate_size(const ce_gen_spec* spec, size_t first, size_t count, size_t* nodes,
+                           size_t* bones, size_t* muscles);
 /* Writes `count` creatures: creature i is a function of (seed, first + i). */
 ce_status ce_generate(const ce_gen_spec* spec, size_t first, size_t count, ce_node_gene* nodes,
                       ce_bone_gene* bones, ce_muscle_gene* muscles, float* strength_scale,
@@ -229,6 +230,13 @@ typedef struct ce_metrics {
 /* scheduler::to_metrics for one result (src/scheduler.rs:859-923). */
 ce_status ce_to_metrics(const ce_result* r, uint32_t node_count, const ce_world* world,
                         ce_metrics* out);
+/* ce_to_metrics for n results; node_counts[i] is result i's node count. */
+ce_status ce_to_metrics_batch(const ce_result* r, const uint32_t* node_counts, size_t n,
+                              const ce_world* world, ce_metrics* out);
+/* ce_niche for creature indices[i] of `pop` with metrics m[i] (indices NULL:
+ * creature i); cells[i] receives the dense cell or -1. */
+ce_status ce_niche_batch(const ce_population* pop, const uint32_t* indices, size_t n,
+                         const ce_metrics* m, int global_layout, int64_t* cells);
 /* qd::descriptor + Descriptor::niche_in + cell_index (src/qd.rs:762-846,
  * 988-999): the dense cell of a creature in the global (global != 0) or
  * island layout, -1 outside the grid. */
@@ -283,6 +291,11 @@ ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const fl
                             void* scratch, const ce_params* params, uint32_t world_flags,
                             uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
                             void* stream);
+
+/* The FP32 multiply-add rate of `device` in TFLOP/s (two operations per
+ * multiply-add), from a calibration kernel of independent chains on every
+ * multiprocessor; the denominator of the creature kernel's FP32 roofline. */
+ce_status ce_measure_fp32(int device, double* tflops, double* seconds);
 
 /* Host-side fault injection for the recovery paths (src/scheduler.rs:725):
  * the `after`-th next submit fails with `status`. 0 turns it off. */

@@ -70,3 +70,49 @@ class RefKernel:
         if rc != 0:
             raise RuntimeError(f"reference kernel failed: {err.value.decode()}")
         return fr, out
+
+
+class Oracle:
+    """The CPU oracle (oracle/creature_oracle.cpp): the reference kernel's
+    per-creature simulation restated on the host, FP32 or FP64."""
+
+    def __init__(self):
+        path = REF / "liboracle.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is missing: build it with python oracle/build_ref.py")
+        self.lib = C.CDLL(str(path))
+        self.lib.oracle_run.restype = C.c_double
+        self.lib.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p,
+                                        C.c_uint32, C.c_int, C.c_int, C.c_void_p, C.c_int]
+        self.lib.oracle_trace.restype = None
+        self.lib.oracle_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32,
+                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]
+        self.lib.oracle_count.restype = None
+        self.lib.oracle_count.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32,
+                                          C.c_int, C.c_void_p, C.c_void_p]
+
+    def run(self, wave, params, flags: int, rate: int = 60, first: int = 0, n: int = None, fp64: bool = False,
+            threads: int = 0):
+        """(results of packed creatures [first, first + n), wall seconds)."""
+        n = len(wave) - first if n is None else n
+        out = np.zeros(n, RESULT_DTYPE)
+        secs = self.lib.oracle_run(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data, first,
+                                   n, C.byref(params), flags, rate, 1 if fp64 else 0, out.ctypes.data, threads)
+        return out, secs
+
+    def trace(self, wave, params, flags: int, cidx: int, steps: int, rate: int = 60, fp64: bool = False):
+        """(result, node positions after every step [steps, 32, 2]) of packed creature `cidx`."""
+        out = np.zeros(1, RESULT_DTYPE)
+        tr = np.full((steps, 32, 2), np.nan, np.float32)
+        self.lib.oracle_trace(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data, cidx,
+                              C.byref(params), flags, rate, 1 if fp64 else 0, out.ctypes.data, tr.ctypes.data, steps)
+        return out[0], tr
+
+    def count(self, wave, params, flags: int, cidx: int, rate: int = 60):
+        """(result, arithmetic counts: add, mul, div, sqrt, transcendental,
+        min/max, compare, other) of packed creature `cidx`'s trial."""
+        out = np.zeros(1, RESULT_DTYPE)
+        counts = np.zeros(8, np.uint64)
+        self.lib.oracle_count(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data, cidx,
+                              C.byref(params), flags, rate, out.ctypes.data, counts.ctypes.data)
+        return out[0], counts
