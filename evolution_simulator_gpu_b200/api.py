@@ -166,6 +166,9 @@ def _bind(lib: C.CDLL) -> None:
                                         C.c_void_p]),
         "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
         "ce_measure_fp32": (C.c_int, [C.c_int, P(C.c_double), P(C.c_double)]),
+        "ce_ground": (None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P(C.c_float),
+                             P(C.c_float)]),
+        "ce_quake_hash": (C.c_uint32, [C.c_uint64]),
         "ce_to_metrics_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
     }
@@ -190,7 +193,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
             "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
-            "ce_to_metrics_batch", "ce_niche_batch"]
+            "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash"]
 
 
 def _check(status: int, what: str) -> None:
@@ -561,6 +564,18 @@ def niche_cells(pop: Population, metrics: np.ndarray, indices=None, global_layou
     _check(lib().ce_niche_batch(C.byref(pc), _ptr(idx), n, m.ctypes.data, 1 if global_layout else 0,
                                 cells.ctypes.data), "ce_niche_batch")
     return cells
+
+
+def ground(x: float, amplitude: float = 0.0, tilt: float = 0.0, width: float = 0.0, hurdle: float = 0.0,
+           phase: float = 0.0):
+    """(height, slope) of the ground under x (physics::ground)."""
+    h, s = C.c_float(), C.c_float()
+    lib().ce_ground(x, amplitude, tilt, width, hurdle, phase, C.byref(h), C.byref(s))
+    return h.value, s.value
+
+
+def quake_hash(creature_id: int) -> int:
+    return int(lib().ce_quake_hash(creature_id))
 
 
 def measure_fp32(device: int = 0) -> float:

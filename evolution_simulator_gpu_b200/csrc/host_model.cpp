@@ -899,3 +899,13 @@ extern "C" ce_status ce_niche_batch(const ce_population* pop, const uint32_t* in
     }
     return CE_OK;
 }
+
+extern "C" void ce_ground(float x, float amplitude, float tilt, float width, float hurdle, float phase, float* height,
+                          float* slope) {
+    float h = 0.0f, sl = 0.0f;
+    ce::ground(x, amplitude, tilt, width, hurdle, phase, h, sl);
+    if (height) *height = h;
+    if (slope) *slope = sl;
+}
+
+extern "C" uint32_t ce_quake_hash(uint64_t id) { return ce::quake_hash(id); }

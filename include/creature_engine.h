@@ -193,6 +193,15 @@ ce_status ce_pack_size(const ce_population* pop, const uint32_t* indices, size_t
 ce_status ce_pack(const ce_population* pop, const uint32_t* indices, size_t n, const ce_world* world,
                   uint32_t* lanes, float* muscles, uint32_t* heads, uint32_t* slots, uint32_t* info);
 
+/* The ground's height and slope under x for bump height `amplitude`, slope
+ * `tilt`, pit width `width`, hurdle height `hurdle` and quake phase `phase`
+ * (physics::ground, src/physics.rs:668-683), as the packer places creatures
+ * on it. */
+void ce_ground(float x, float amplitude, float tilt, float width, float hurdle, float phase,
+               float* height, float* slope);
+/* The quake hash of a creature id (physics::quake_hash, src/physics.rs:640-648). */
+uint32_t ce_quake_hash(uint64_t id);
+
 /* Frame slots of a recording (src/creature_kernel.rs:312-326). */
 uint32_t ce_frame_stride(uint32_t max_muscles);
 

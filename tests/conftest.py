@@ -18,6 +18,15 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 GPU")
+    # A fresh checkout has no built libraries: build the engine and the
+    # checkers (the reference kernel only where the reference checkout is).
+    from evolution_simulator_gpu_b200 import api
+    if not api.LIB_PATH.exists():
+        from evolution_simulator_gpu_b200.build import build
+        build()
+    if not (ROOT / "oracle" / "_ref" / "liboracle.so").exists():
+        from oracle.build_ref import build as build_checkers
+        build_checkers()
 
 
 def gpu_available() -> bool:
