@@ -169,6 +169,9 @@ def _bind(lib: C.CDLL) -> None:
         "ce_ground": (None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P(C.c_float),
                              P(C.c_float)]),
         "ce_quake_hash": (C.c_uint32, [C.c_uint64]),
+        "ce_advance_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(Params),
+                                                C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]),
+        "ce_noalloc_scratch_bytes": (C.c_size_t, []),
         "ce_to_metrics_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
     }
@@ -193,7 +196,8 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
             "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
-            "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash"]
+            "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
+            "ce_noalloc_scratch_bytes"]
 
 
 def _check(status: int, what: str) -> None:

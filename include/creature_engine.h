@@ -301,6 +301,22 @@ ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const fl
                             uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
                             void* stream);
 
+/* The device-level entry above for a caller that cannot allocate GPU memory:
+ * no counterpart in the reference. It allocates nothing: the kernel's
+ * scratch (claim counter and lane slots) is a fixed array of
+ * ce_noalloc_scratch_bytes() (32 MiB) in the library's device memory, held
+ * on every GPU that loads the library until exit. It runs on the current
+ * device, as many warps as the array holds at this body size (so it can be
+ * slower than ce_advance_device), and rejects a body size whose single block
+ * does not fit. Calls share the array: calls that overlap on the GPU race.
+ * The first call on a device resolves the array's address there and must
+ * come before any stream capture. Inputs and outputs are the caller's. */
+ce_status ce_advance_device_noalloc(const uint32_t* records, const float* muscles,
+                                    const uint32_t* heads, ce_result* results,
+                                    const ce_params* params, uint32_t world_flags, uint32_t rate,
+                                    uint32_t max_nodes, uint32_t max_muscles, void* stream);
+size_t ce_noalloc_scratch_bytes(void);
+
 /* The FP32 multiply-add rate of `device` in TFLOP/s (two operations per
  * multiply-add), from a calibration kernel of independent chains on every
  * multiprocessor; the denominator of the creature kernel's FP32 roofline. */
