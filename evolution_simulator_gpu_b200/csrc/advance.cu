@@ -13,16 +13,6 @@ namespace cek {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// The ground under a node for the step's contact tallies, as a call rather
-// than inlined: the reference kernel's tallies compute the ground through a
-// call too, and only with the same call boundary do the contact tests round
-// the same (an inlined ground lets the compiler fuse the floor height's
-// multiply-add with the ground's last term, which moves a contact test at
-// its edge by one unit in the last place).
-template <class W>
-__device__ __noinline__ float2 ground_call(const W& w, float x, float amp, float qphase, const ce_params& p) {
-    return ground(w, x, amp, qphase, p);
-}
 
 template <class W, bool RECORD, int RATE>
 struct Trial {
@@ -187,8 +177,8 @@ struct Trial {
             low = fminf(low, q.y - nr.z);
             high = fmaxf(high, q.y + nr.z);
             if (b.w.has(CE_FLAG_GROUND)) {
-                const float2 g = ground_call(b.w, q.x, r.amp, r.qphase, p);
-                const float floor_y = g.x + nr.z * sqrtf(1.0f + g.y * g.y);
+                const float2 g = ground_tally(b.w, q.x, r.amp, r.qphase, p);
+                const float floor_y = __fmaf_rn(nr.z, sqrtf(__fmaf_rn(g.y, g.y, 1.0f)), g.x);
                 if (q.y <= floor_y + kContactSlack) {
                     touching |= 1u << i;
                 }

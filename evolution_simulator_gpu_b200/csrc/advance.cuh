@@ -196,8 +196,11 @@ struct Creature {
     // Air and water drag on the bones (shaders/creature.cu:553-593).
     __device__ __forceinline__ void bone_drag() const {
         const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.bone), nb = L.get(S.bone + 1u);
         for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = L.get(S.bone + 2u * j), bb = L.get(S.bone + 2u * j + 1u);
+            const float4 ba = na, bb = nb;
+            na = L.get(S.bone + 2u * j + 2u);
+            nb = L.get(S.bone + 2u * j + 3u);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float2 v0 = t.vel(i0), v1 = t.vel(i1);
             const float wx = 0.5f * (v0.x + v1.x), wy = 0.5f * (v0.y + v1.y);
@@ -231,8 +234,10 @@ struct Creature {
     // Bone lengths (shaders/creature.cu:597-613).
     __device__ __forceinline__ void solve_bones() const {
         const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.bone);
         for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = L.get(S.bone + 2u * j);
+            const float4 ba = na;
+            na = L.get(S.bone + 2u * j + 2u);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float2 p0 = t.pos(i0), p1 = t.pos(i1);
             const float dx = p1.x - p0.x, dy = p1.y - p0.y;
@@ -249,8 +254,11 @@ struct Creature {
     // Joint ranges (shaders/creature.cu:618-634).
     __device__ __forceinline__ void solve_joints() const {
         const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
         for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = na, rb = nb;
+            na = L.get(S.joint + 2u * j + 2u);
+            nb = L.get(S.joint + 2u * j + 3u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }
@@ -317,8 +325,11 @@ struct Creature {
     __device__ __forceinline__ void damp_joints() const {
         const float share = fminf(C::h * kInvJointDamping, 1.0f);
         const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
         for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = na, rb = nb;
+            na = L.get(S.joint + 2u * j + 2u);
+            nb = L.get(S.joint + 2u * j + 3u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }
@@ -337,8 +348,10 @@ struct Creature {
     __device__ __forceinline__ void substep() const {
         muscle_forces();
         bone_drag();
+        float4 nn = L.get(S.node);
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
+            const float4 nr = nn;
+            nn = L.get(S.node + i + 1u);
             const float2 f = node_force(i, nr);
             float4 s = t.at(i);
             const float2 fpv = t.f(i);
@@ -355,8 +368,10 @@ struct Creature {
         }
         solve_bones();
         solve_joints();
+        nn = L.get(S.node);
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
+            const float4 nr = nn;
+            nn = L.get(S.node + i + 1u);
             solve_ground(i, nr);
             const float2 q = t.pos(i), f0 = t.f(i);
             t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
@@ -369,8 +384,11 @@ struct Creature {
     __device__ __forceinline__ unsigned long long broken_joints() const {
         unsigned long long bits = 0ull;
         const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
         for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = na, rb = nb;
+            na = L.get(S.joint + 2u * j + 2u);
+            nb = L.get(S.joint + 2u * j + 3u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }

@@ -150,6 +150,74 @@ __device__ __forceinline__ float2 ground(const W& w, float x, float amp, float q
     return make_float2(height, slope);
 }
 
+
+// The ground and floor height of the step's contact tallies with every
+// rounding pinned (fused multiply-adds where the reference kernel's compiled
+// tallies fuse them, measured on the GPU), so no other code change can move
+// the contact tests at their edges.
+template <class W>
+__device__ __forceinline__ float2 ground_tally(const W& w, float x, float amp, float qphase, const ce_params& p) {
+    float height = 0.0f, slope = 0.0f;
+    if (w.has(CE_FLAG_TERRAIN)) {
+        const float t0 = __fmaf_rn(x, (1.0f / 1.1f), qphase);
+        const float u0 = __fsub_rn(t0, floorf(t0));
+        const float w0 = __fmul_rn(u0, __fsub_rn(1.0f, u0));
+        const float t1 = __fadd_rn(__fmaf_rn(x, (1.0f / 0.43f), 0.3f), qphase);
+        const float u1 = __fsub_rn(t1, floorf(t1));
+        const float w1 = __fmul_rn(u1, __fsub_rn(1.0f, u1));
+        height = __fmul_rn(amp, __fmaf_rn(__fmul_rn(0.65f * 16.0f, w0), w0, __fmul_rn(__fmul_rn(0.35f * 16.0f, w1), w1)));
+        const float a2 = __fmul_rn(__fmul_rn(0.65f * 32.0f, w0), __fsub_rn(1.0f, __fmul_rn(2.0f, u0)));
+        const float b2 = __fmul_rn(__fmul_rn(0.35f * 32.0f, w1), __fsub_rn(1.0f, __fmul_rn(2.0f, u1)));
+        slope = __fmaf_rn(a2, (1.0f / 1.1f), __fmul_rn(b2, (1.0f / 0.43f)));
+        if (w.has(CE_FLAG_SLOPE)) {
+            height = __fmaf_rn(p.slope, x, height);
+            slope = __fmaf_rn(amp, slope, p.slope);
+        } else {
+            slope = __fmul_rn(amp, slope);
+        }
+    } else if (w.has(CE_FLAG_SLOPE)) {
+        height = __fmul_rn(p.slope, x);
+        slope = p.slope;
+    }
+    if (w.has(CE_FLAG_GAPS)) {
+        const float spacing = __fmaf_rn(4.0f, p.gaps, 2.0f);
+        const float center = __fmul_rn(spacing, 0.5f);
+        const float r = __fmaf_rn(-floorf(x / spacing), spacing, x);
+        const float distance = fabsf(__fsub_rn(r, center));
+        const float half_w = __fmul_rn(0.5f, p.gaps);
+        const float run = fmaxf(fminf(kGapRun, half_w), 1e-6f);
+        float factor = clampf(__fsub_rn(half_w, distance) / run, 0.0f, 1.0f);
+        if (distance <= __fsub_rn(half_w, run)) {
+            factor = 1.0f;
+        } else if (distance >= half_w) {
+            factor = 0.0f;
+        }
+        height = __fmaf_rn(-kGapDepth, factor, height);
+        if (distance > __fsub_rn(half_w, run) && distance < half_w) {
+            slope = __fmaf_rn(-kGapDepth, (r < center ? 1.0f : -1.0f) / run, slope);
+        }
+    }
+    if (w.has(CE_FLAG_HURDLES)) {
+        const float spacing = kHurdleSpacing;
+        const float center = spacing * 0.5f;
+        const float r = __fmaf_rn(-floorf(x / spacing), spacing, x);
+        const float distance = fabsf(__fsub_rn(r, center));
+        const float half_w = 0.5f * kHurdleTop;
+        const float run = kHurdleRun;
+        float factor = clampf((half_w + run - distance) / run, 0.0f, 1.0f);
+        if (distance <= half_w) {
+            factor = 1.0f;
+        } else if (distance >= half_w + run) {
+            factor = 0.0f;
+        }
+        height = __fmaf_rn(p.hurdles, factor, height);
+        if (distance > half_w && distance < half_w + run) {
+            slope = __fmaf_rn(p.hurdles, (r < center ? 1.0f : -1.0f) / run, slope);
+        }
+    }
+    return make_float2(height, slope);
+}
+
 // Ice at x (shaders/creature.cu:230-235).
 __device__ __forceinline__ float ice_at(float x) {
     const float w = fracf(x * kIceInv);
@@ -192,6 +260,12 @@ struct Lines {
 // MM muscles at most. A recording slot also has a line per node for its
 // contact forces (`rec_force`), the kept result (`rec_kept`, 5 lines) and
 // the muscles' pulls, four to a line (`rec_pull`).
+//
+// The node, bone and joint passes load the line of the next item while they
+// work on the current one, so each loads one item past its last. The
+// regions follow each other (nodes, bones, joints, muscles, then the nine
+// lane lines), so that extra load always lands inside the lane's own slot;
+// a layout that ends with one of those regions needs padding after it.
 struct SlotLayout {
     unsigned node, bone, joint, muscle, lane, rec_force, rec_kept, rec_pull, lines;
     __host__ __device__ static SlotLayout make(unsigned ns, unsigned mm, bool record) {
