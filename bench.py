@@ -159,15 +159,6 @@ def build_workload(n: int, rank: int):
     return world, pop, wave
 
 
-def substeps_run(results: np.ndarray, world) -> float:
-    import evolution_simulator_gpu_b200 as ce
-    rate = world.rate or 60
-    total = ce.trial_steps(world)
-    t = np.where(results["fall_time"] > 0, results["fall_time"] * rate,
-                 np.where(results["screened"] > 0, results["screened"] * rate, total))
-    return float(16.0 * np.minimum(np.round(t), total).sum())
-
-
 def op_counts() -> dict:
     path = ROOT / "profiles" / "op_counts.json"
     return json.loads(path.read_text()) if path.exists() else {}
@@ -181,10 +172,13 @@ def traffic_per_substep():
 
 
 # ---------------------------------------------------------------- CPU baseline
-def cpu_baseline(wave, world, budget_s: float) -> dict:
+def cpu_sample(wave, world, budget_s: float, phase: int = 0):
     """The CPU oracle (oracle/creature_oracle.cpp, FP32, all host threads) on a
-    bounded sample of the same generation: creatures in packed order from
-    evenly spread chunks until `budget_s` of wall time."""
+    bounded sample of the generation: chunks of 64 creatures per thread taken
+    from 64 evenly spread places of the packed order (which is sorted by size,
+    so the sample spans every size), shifted by `phase` chunks so repeated
+    samples differ, until `budget_s` seconds of oracle time. Returns
+    (creature-substeps, seconds, creatures, threads)."""
     import evolution_simulator_gpu_b200 as ce
     from oracle.ref import Oracle
     oracle = Oracle()
@@ -192,17 +186,23 @@ def cpu_baseline(wave, world, budget_s: float) -> dict:
     flags = ce.world_flags(world)
     cores = os.cpu_count() or 1
     n = len(wave)
-    chunk = 64 * cores
+    chunk = min(64 * cores, n)
     starts = np.linspace(0, n - chunk, 64).astype(np.int64)
+    starts = (starts + phase * chunk) % (n - chunk + 1)
     done = secs = 0.0
     creatures = 0
     for s in starts:
         res, t = oracle.run(wave, params, flags, world.rate or 60, int(s), chunk, threads=cores)
         secs += t
-        done += substeps_run(res, world)
+        done += ce.creature_substeps(res, world)
         creatures += chunk
         if secs > budget_s:
             break
+    return done, secs, creatures, cores
+
+
+def cpu_baseline(wave, world, budget_s: float) -> dict:
+    done, secs, creatures, cores = cpu_sample(wave, world, budget_s)
     return {"value": done / secs, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{creatures} creatures of the same generation (chunks spread over the packed order), "
                       f"{done:.3g} creature-substeps in {secs:.1f} s"}
@@ -241,7 +241,7 @@ def run_engine(args):
         one_step()
     torch.cuda.synchronize(dev)
     res = d_results.cpu().numpy().view(ce.RESULT_DTYPE)
-    units = substeps_run(res, world)
+    units = ce.creature_substeps(res, world)
     clocks = ClockSampler(local)
     clocks.start()
     barrier(world_size)
@@ -277,7 +277,7 @@ def run_engine(args):
         e2e_launches += 1 if wave.max_nodes <= 16 else 2
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, world_size)
-    e2e_value = sum_over_ranks(substeps_run(out, world) * args.steps, world_size) / e2e_s
+    e2e_value = sum_over_ranks(ce.creature_substeps(out, world) * args.steps, world_size) / e2e_s
     same = bool((out.view(np.uint32) == res.view(np.uint32)).all())
 
     if rank == 0:
@@ -329,34 +329,20 @@ def run_reference(args):
     if rank != 0:
         return
     import evolution_simulator_gpu_b200 as ce
-    from oracle.ref import Oracle, RefKernel
+    from oracle.ref import RefKernel
     world, pop, wave = build_workload(args.creatures, 0)
-    oracle = Oracle()
     params = ce.make_params(world)
     flags = ce.world_flags(world)
-    cores = os.cpu_count() or 1
-    chunk = 32 * cores
-    n = len(wave)
-    rng = np.random.default_rng(0)
     per_step = max(args.cpu_seconds / 4.0, 2.0)
-
-    def one_step():
-        done = secs = 0.0
-        count = 0
-        while secs < per_step:
-            s = int(rng.integers(0, n - chunk))
-            res, t = oracle.run(wave, params, flags, world.rate or 60, s, chunk, threads=cores)
-            secs += t
-            done += substeps_run(res, world)
-            count += chunk
-        return done, secs, count
-
+    phase = 0
     for _ in range(args.warmup):
-        one_step()
+        cpu_sample(wave, world, per_step, phase)
+        phase += 1
     tot_units = tot_secs = 0.0
     tot_count = 0
     for _ in range(args.steps):
-        u, s, c = one_step()
+        u, s, c, cores = cpu_sample(wave, world, per_step, phase)
+        phase += 1
         tot_units += u
         tot_secs += s
         tot_count += c
@@ -366,18 +352,19 @@ def run_reference(args):
         kern = RefKernel(flags, world.rate or 60)
         kern.run(wave.take(np.arange(4096)), params)
         res, ms = kern.run(wave, params)
-        ref_gpu = {"value": substeps_run(res, world) / (ms / 1e3), "unit": UNIT,
+        ref_gpu = {"value": ce.creature_substeps(res, world) / (ms / 1e3), "unit": UNIT,
                    "what": "the reference's own kernel (shaders/creature.cu) built for sm_100a with its NVRTC "
                            "options, launched with its engine's wave and grid rule, CUDA-event time of one "
                            "generation", "seconds": ms / 1e3}
     except Exception as exc:  # the reference kernel needs a GPU
         ref_gpu = {"unavailable": str(exc).splitlines()[0]}
-    sample = f"{tot_count} creatures of the generation in chunks of {chunk}, {tot_units:.3g} creature-substeps"
+    sample = (f"{tot_count} creatures of the generation (chunks spread over the packed order), "
+              f"{tot_units:.3g} creature-substeps in {tot_secs:.1f} s")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD_TEXT, "creatures_per_gpu": n},
+            "config": {"workload": WORKLOAD_TEXT, "creatures_per_gpu": len(wave)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "reference_gpu": ref_gpu}

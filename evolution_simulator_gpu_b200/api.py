@@ -262,6 +262,17 @@ def trial_steps(w: World) -> int:
     return int(np.round(np.float32(w.duration) * np.float32(w.rate or 60)))
 
 
+def creature_substeps(results: np.ndarray, w: World) -> float:
+    """Substeps the trials of `results` ran: a creature stops at its fall
+    (fall_time) or at the screen (screened), else runs the whole trial, 16
+    substeps a step (shaders/creature.cu:1063, 1159, 1182)."""
+    rate = w.rate or 60
+    total = trial_steps(w)
+    t = np.where(results["fall_time"] > 0, results["fall_time"] * rate,
+                 np.where(results["screened"] > 0, results["screened"] * rate, total))
+    return float(SUBSTEPS * np.minimum(np.round(t), total).sum())
+
+
 # -------------------------------------------------------------- population
 @dataclasses.dataclass
 class Population:

@@ -5,7 +5,8 @@ of the engine against the reference kernel on the same case.
         --creatures 300000 --seconds 1 [--reference]
 
 It generates the workload, runs one submission through the engine (one
-launch per size class) and prints the GPU seconds. With --reference it also
+launch per size class) and prints the GPU seconds, the creature-substeps the
+trials ran and the bytes of the packed records. With --reference it also
 runs the reference's own kernel (oracle/_ref, built from its source) on the
 same batch and prints whether the results are equal to the bit.
 """
@@ -36,7 +37,9 @@ def main() -> None:
     wave = ce.pack(pop, world)
     with ce.Engine(0) as eng:
         mine, busy = eng.run(wave, world)
-    out = {"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds, "engine_s": busy}
+    out = {"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds, "engine_s": busy,
+           "creature_substeps": ce.creature_substeps(mine, world),
+           "record_bytes": int(wave.lanes.nbytes + wave.muscles.nbytes + wave.heads.nbytes)}
     if args.reference:
         sys.path.insert(0, str(ROOT))
         from oracle.ref import RefKernel
