@@ -160,7 +160,8 @@ def _bind(lib: C.CDLL) -> None:
         "ce_allocated_bytes": (C.c_size_t, [C.c_void_p]),
         "ce_release_idle": (C.c_int, [C.c_void_p]),
         "ce_record": (C.c_int, [C.c_void_p, P(WavePackC), P(World), C.c_void_p, C.c_size_t, C.c_void_p]),
-        "ce_advance_scratch_bytes": (C.c_size_t, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+        "ce_advance_scratch_bytes": (C.c_size_t, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                  C.c_uint32]),
         "ce_advance_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, P(Params), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p]),
@@ -536,8 +537,9 @@ class Engine:
                                _ptr(res)), "ce_record")
         return frames, res
 
-    def scratch_bytes(self, flags: int, rate: int, max_nodes: int, max_muscles: int) -> int:
-        return int(lib().ce_advance_scratch_bytes(self.handle, flags, rate, max_nodes, max_muscles))
+    def scratch_bytes(self, flags: int, rate: int, max_nodes: int, max_muscles: int, count: int) -> int:
+        """Bytes of the scratch of advance_device for `count` creatures."""
+        return int(lib().ce_advance_scratch_bytes(self.handle, flags, rate, max_nodes, max_muscles, count))
 
     def advance_device(self, records: int, muscles: int, heads: int, results: int, counter: int, scratch: int,
                        params: Params, flags: int, rate: int, max_nodes: int, max_muscles: int,

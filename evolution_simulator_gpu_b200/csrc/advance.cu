@@ -45,8 +45,8 @@ struct Trial {
         const ce_params& p = b.p;
         const Lines& L = b.L;
         const SlotLayout& S = b.S;
-        const uint4 h0 = __ldg(&a.heads[2u * cidx]);
-        const uint4 h1 = __ldg(&a.heads[2u * cidx + 1u]);
+        const uint4 h0 = __ldcs(&a.heads[2u * cidx]);
+        const uint4 h1 = __ldcs(&a.heads[2u * cidx + 1u]);
         r.cidx = cidx;
         r.rec_slot = slot;
         r.nodes = h0.x & 255u;
@@ -66,10 +66,10 @@ struct Trial {
         r.feet = 0u;
         for (unsigned i = 0u; i < r.nodes; i++) {
             const uint32_t* q = rec + i * CE_NODE_WORDS;
-            const float m = __uint_as_float(__ldg(q + 0));
-            L.put(S.node + i, make_float4(m, 1.0f / m, __uint_as_float(__ldg(q + 1)), __uint_as_float(__ldg(q + 2))));
-            b.t.at(i) = make_float4(__uint_as_float(__ldg(q + 3)), __uint_as_float(__ldg(q + 4)), 0.0f, 0.0f);
-            r.feet |= (__ldg(q + 5) & 1u) << i;
+            const float m = __uint_as_float(__ldcs(q + 0));
+            L.put(S.node + i, make_float4(m, 1.0f / m, __uint_as_float(__ldcs(q + 1)), __uint_as_float(__ldcs(q + 2))));
+            b.t.at(i) = make_float4(__uint_as_float(__ldcs(q + 3)), __uint_as_float(__ldcs(q + 4)), 0.0f, 0.0f);
+            r.feet |= (__ldcs(q + 5) & 1u) << i;
             if (RECORD) {
                 L.put(S.rec_force + i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
             }
@@ -78,8 +78,8 @@ struct Trial {
         const unsigned bones = r.nodes - 1u;
         for (unsigned j = 0u; j < bones; j++) {
             const uint32_t* q = bone_rec + j * CE_BONE_WORDS;
-            const unsigned i0 = __ldg(q + 0), i1 = j + 1u;
-            const float length = __uint_as_float(__ldg(q + 1));
+            const unsigned i0 = __ldcs(q + 0), i1 = j + 1u;
+            const float length = __uint_as_float(__ldcs(q + 1));
             const float4 n0 = L.get(S.node + i0), n1 = L.get(S.node + i1);
             const float width = n0.z + n1.z;
             const float bone_mass = n0.x + n1.x;
@@ -88,14 +88,14 @@ struct Trial {
                                                     0.5f * C::h * n0.y, 0.5f * C::h * n1.y));
             float4 ra = make_float4(__uint_as_float(kNone), 0.0f, 0.0f, 0.0f);
             float4 rb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            const unsigned pj = __ldg(q + 2);
+            const unsigned pj = __ldcs(q + 2);
             if (j > 0u && pj != kNone) {
-                const unsigned hub = i0, parent_pivot = __ldg(bone_rec + pj * CE_BONE_WORDS);
+                const unsigned hub = i0, parent_pivot = __ldcs(bone_rec + pj * CE_BONE_WORDS);
                 const bool at_head = hub == parent_pivot;
                 const unsigned far = at_head ? pj + 1u : parent_pivot;
                 const unsigned topo =
                     hub | ((pj + 1u) << 5u) | (parent_pivot << 10u) | (far << 15u) | ((at_head ? 1u : 0u) << 20u);
-                const float lo = __uint_as_float(__ldg(q + 3)), hi = __uint_as_float(__ldg(q + 4));
+                const float lo = __uint_as_float(__ldcs(q + 3)), hi = __uint_as_float(__ldcs(q + 4));
                 ra = make_float4(__uint_as_float(topo), lo, hi, 0.5f * (lo + hi));
                 rb = make_float4(n1.y, L.get(S.node + far).y, n0.y, 0.0f);
             }
@@ -105,26 +105,31 @@ struct Trial {
         for (unsigned k = 0u; k < r.muscles; k++) {
             const float4* q = reinterpret_cast<const float4*>(mus + k * CE_MUSCLE_FIELDS);
             const unsigned m0 = S.muscle + 5u * k;
-            L.put(m0 + kPull0, __ldg(q + 0));
-            L.put(m0 + kPull1, __ldg(q + 1));
-            L.put(m0 + kRhythm0, __ldg(q + 2));
-            L.put(m0 + kRhythm1, __ldg(q + 3));
-            L.put(m0 + kMState, make_float4(0.0f, 0.0f, 0.0f, __ldg(q + 4).x));
+            L.put(m0 + kPull0, __ldcs(q + 0));
+            L.put(m0 + kPull1, __ldcs(q + 1));
+            L.put_cold(m0 + kRhythm0, __ldcs(q + 2));
+            L.put_cold(m0 + kRhythm1, __ldcs(q + 3));
+            L.put_cold(m0 + kMState, make_float4(0.0f, 0.0f, 0.0f, __ldcs(q + 4).x));
             b.t.muscle(k) = make_float2(1.0f, 0.0f);
             if (RECORD) {
                 L.word(S.rec_pull + k / 4u, k % 4u) = 0.0f;
             }
         }
         // The result starts at 0 except the lowest and highest mean height.
-        for (unsigned q = 0u; q < 8u; q++) {
-            L.put(S.lane + q, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
-        }
-        L.put(S.lane + 8u, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
-        L.word(S.lane, 2) = 1e20f;
-        L.word(S.lane, 3) = -1e20f;
         const float2 head = b.t.pos(0u);
-        L.word(S.lane + kWHeadAt / 4u, kWHeadAt % 4u) = head.x;
-        L.word(S.lane + (kWHeadAt + 1u) / 4u, (kWHeadAt + 1u) % 4u) = head.y;
+        float lw[36];
+#pragma unroll
+        for (unsigned q = 0u; q < 36u; q++) {
+            lw[q] = 0.0f;
+        }
+        lw[2] = 1e20f;
+        lw[3] = -1e20f;
+        lw[kWHeadAt] = head.x;
+        lw[kWHeadAt + 1u] = head.y;
+#pragma unroll
+        for (unsigned q = 0u; q < 9u; q++) {
+            L.put_cold(S.lane + q, make_float4(lw[4u * q], lw[4u * q + 1u], lw[4u * q + 2u], lw[4u * q + 3u]));
+        }
         r.limp = false;
         r.scoring = true;
         r.step = 0u;
@@ -190,11 +195,18 @@ struct Trial {
         center_y /= (float)r.nodes;
         com_x *= r.inv_mass;
         // The result and tallies, from the lane lines.
-        float m[19];
-        for (unsigned q = 0u; q < 19u; q++) {
-            m[q] = L.word(S.lane + q / 4u, q % 4u);
+        // Words 0-18 are the result, 19-31 the tallies.
+        float lw[32];
+#pragma unroll
+        for (unsigned q = 0u; q < 8u; q++) {
+            const float4 v = L.get_cold(S.lane + q);
+            lw[4u * q] = v.x;
+            lw[4u * q + 1u] = v.y;
+            lw[4u * q + 2u] = v.z;
+            lw[4u * q + 3u] = v.w;
         }
-        auto LW = [&](unsigned q) -> float& { return L.word(S.lane + q / 4u, q % 4u); };
+        float* const m = lw;
+        auto LW = [&](unsigned q) -> float& { return lw[q]; };
         unsigned contact_bits = __float_as_uint(LW(kWContact));
         unsigned lift_bits = __float_as_uint(LW(kWLift));
         unsigned ground_bits = __float_as_uint(LW(kWGround));
@@ -234,10 +246,10 @@ struct Trial {
             const float next = t_now + C::dt;
             for (unsigned k = 0u; k < r.muscles; k++) {
                 const unsigned m0 = S.muscle + 5u * k;
-                const unsigned sensor = __float_as_uint(L.word(m0 + kMState, 3));
+                const unsigned sensor = __float_as_uint(L.word_cold(m0 + kMState, 3));
                 if (sensor != kNone && ((down >> sensor) & 1u)) {
-                    const float4 r0 = L.get(m0 + kRhythm0), r1 = L.get(m0 + kRhythm1);
-                    L.word(m0 + kMState, 2) = fracf(r1.w - (next * r0.y + r0.z));
+                    const float4 r0 = L.get_cold(m0 + kRhythm0), r1 = L.get_cold(m0 + kRhythm1);
+                    L.set_cold(m0 + kMState, 2, fracf(r1.w - (next * r0.y + r0.z)));
                 }
             }
         }
@@ -410,7 +422,7 @@ struct Trial {
                 } else {
                     float* out = reinterpret_cast<float*>(a.results + r.cidx);
                     for (unsigned q = 0u; q < 19u; q++) {
-                        out[q] = m[q];
+                        __stcs(out + q, m[q]);
                     }
                     done = true;
                 }
@@ -418,9 +430,6 @@ struct Trial {
         }
         if (done) {
             return false;
-        }
-        for (unsigned q = 0u; q < 19u; q++) {
-            L.word(S.lane + q / 4u, q % 4u) = m[q];
         }
         LW(kWContact) = __uint_as_float(contact_bits);
         LW(kWLift) = __uint_as_float(lift_bits);
@@ -435,6 +444,10 @@ struct Trial {
         LW(kWRungEarly) = __uint_as_float(rung_early);
         LW(kWRungLate) = __uint_as_float(rung_late);
         LW(kWRungBits) = __uint_as_float(rung_bits);
+#pragma unroll
+        for (unsigned q = 0u; q < 8u; q++) {
+            L.put_cold(S.lane + q, make_float4(lw[4u * q], lw[4u * q + 1u], lw[4u * q + 2u], lw[4u * q + 3u]));
+        }
         if (RECORD) {
             record_frame(b, a, C::settle + step + 1u);
             if (step + 1u >= p.steps) {
@@ -470,6 +483,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const Kerne
     unsigned win_cur = 0u, win_end = 0u;
     bool drained = false;
     const unsigned below = (1u << lane) - 1u;
+    // The warp's queue: the warps split between the queues by estimated
+    // work, and a warp whose queue runs dry moves on to the next one.
+    const unsigned queues = a.queues > 0u ? a.queues : 1u;
+    unsigned long long total_work = 1ull;
+    unsigned queue = 0u;
+    if (a.queues > 1u) {
+        total_work = max(a.work[a.queues] - a.work[0], 1ull);
+        const unsigned long long target =
+            a.work[0] + total_work * (2ull * warp + 1ull) / (2ull * warps_total);
+        while (queue + 1u < a.queues && a.work[queue + 1u] <= target) {
+            queue++;
+        }
+    }
     for (;;) {
         unsigned need = ~__ballot_sync(kFull, live);
         unsigned mine = kNone;
@@ -478,21 +504,40 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const Kerne
                 if (drained) {
                     break;
                 }
-                unsigned c0 = 0u, want = 0u;
+                unsigned c0 = kNone, c1 = 0u, got_queue = queue;
                 if (lane == 0u) {
-                    const unsigned seen = *reinterpret_cast<volatile unsigned*>(a.counter);
-                    const unsigned left = seen < a.count ? a.count - seen : 0u;
-                    want = min(max(left / (a.chunk_k * warps_total), 1u), kChunk);
-                    c0 = atomicAdd(a.counter, want);
+                    for (unsigned t = 0u; t < queues; t++) {
+                        const unsigned q = queue + t < queues ? queue + t : queue + t - queues;
+                        const unsigned lo = a.queues > 0u ? a.bounds[q] : 0u;
+                        const unsigned n = (a.queues > 0u ? a.bounds[q + 1u] : a.count) - lo;
+                        const unsigned seen = *reinterpret_cast<volatile unsigned*>(a.counter + q);
+                        if (seen >= n) {
+                            continue;
+                        }
+                        unsigned share = warps_total;
+                        if (a.queues > 1u) {
+                            share = (unsigned)max(1ull, warps_total * (a.work[q + 1u] - a.work[q]) / total_work);
+                        }
+                        const unsigned want = min(max((n - seen) / (a.chunk_k * share), 1u), kChunk);
+                        const unsigned got = atomicAdd(a.counter + q, want);
+                        if (got >= n) {
+                            continue;
+                        }
+                        c0 = lo + got;
+                        c1 = lo + min(got + want, n);
+                        got_queue = q;
+                        break;
+                    }
                 }
                 c0 = __shfl_sync(kFull, c0, 0);
-                want = __shfl_sync(kFull, want, 0);
-                if (c0 >= a.count) {
+                c1 = __shfl_sync(kFull, c1, 0);
+                queue = __shfl_sync(kFull, got_queue, 0);
+                if (c0 == kNone) {
                     drained = true;
                     break;
                 }
                 win_cur = c0;
-                win_end = min(c0 + want, a.count);
+                win_end = c1;
             }
             const unsigned rank = (unsigned)__popc(need & below);
             const bool take = ((need >> lane) & 1u) != 0u && rank < win_end - win_cur;

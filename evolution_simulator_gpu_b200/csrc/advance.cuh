@@ -101,9 +101,9 @@ struct Creature {
     __device__ __forceinline__ void muscle_demands(float t_now) const {
         for (unsigned k = 0u; k < r.muscles; k++) {
             const unsigned m0 = S.muscle + 5u * k;
-            const float4 r0 = L.get(m0 + kRhythm0), r1 = L.get(m0 + kRhythm1);
+            const float4 r0 = L.get_cold(m0 + kRhythm0), r1 = L.get_cold(m0 + kRhythm1);
             float& demand = t.muscle(k).y;
-            const float offset = L.word(m0 + kMState, 2);
+            const float offset = L.word_cold(m0 + kMState, 2);
             const float before = rhythm(t_now, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
             const float after = rhythm(t_now + C::dt, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
             const float shortening = r0.x * (after - before) * C::rate;

@@ -2,10 +2,11 @@
 // each with its stream, events, pinned staging and device buffers.
 //
 // A submission (the reference's CudaEngine::launch, src/cuda_engine.rs:
-// 2106-2316) uploads the packed batch, splits it into two size classes by
-// node count (bodies of at most 16 nodes, and larger ones), runs one
-// persistent launch per class, the two side by side on two streams so that
-// the tail of one overlaps the other, and reads the results back. ce_poll hands back
+// 2106-2316) uploads the packed batch, buckets it by node count on the
+// device into claim queues, splits it into two size classes by node count
+// (bodies of at most 16 nodes, and larger ones), runs one persistent launch
+// per class, the two side by side on two streams so that the tail of one
+// overlaps the other, and reads the results back. ce_poll hands back
 // the oldest finished submission with its GPU-busy seconds, as the
 // reference's poll does (src/cuda_engine.rs:2319-2393).
 #include <cuda_runtime.h>
@@ -86,9 +87,10 @@ struct PinnedBuf {
 };
 
 struct ClassPlan {
-    uint32_t first, count;  // range of the order list
-    uint32_t rows;          // most nodes in the class
-    uint32_t mm;            // most muscles in the class
+    uint32_t first_n, last_n;  // node counts of the class: its claim queues
+    uint32_t count;            // creatures of the class
+    uint32_t rows;             // most nodes in the class
+    uint32_t mm;               // most muscles in the class
 };
 
 struct Slot {
@@ -96,8 +98,8 @@ struct Slot {
     uint64_t ticket = 0;
     size_t count = 0;
     cudaStream_t stream = nullptr, side = nullptr;  // side: the second class
-    cudaEvent_t start = nullptr, stop = nullptr, done = nullptr, joined = nullptr;
-    DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_order, d_counters, d_scratch;
+    cudaEvent_t start = nullptr, stop = nullptr, done = nullptr, joined = nullptr, bucketed = nullptr;
+    DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_buckets, d_scratch;
     PinnedBuf h_upload, h_results;
     std::chrono::steady_clock::time_point submitted;
 };
@@ -159,28 +161,35 @@ ce_status check_world(const ce_world* w) {
     return CE_OK;
 }
 
-// Splits the packed batch into size classes: the order list holds the packed
-// positions of each class in turn, each class in packed order.
-ce_status plan_classes(const ce_wave_pack* pack, std::vector<uint32_t>& order, std::vector<ClassPlan>& plans) {
-    order.clear();
+// Splits the packed batch into size classes by node count (bodies of at most
+// kSmallBody nodes, and larger ones). Each class runs as one launch whose
+// claim queues are its node counts (kernels.h); the bucketing kernels build
+// the queues on the device.
+ce_status plan_classes(const ce_wave_pack* pack, std::vector<ClassPlan>& plans) {
     plans.clear();
-    order.reserve(pack->count);
-    for (int big = 0; big < 2; big++) {
-        ClassPlan c{(uint32_t)order.size(), 0, 2, 0};
-        for (size_t i = 0; i < pack->count; i++) {
-            const uint32_t* h = pack->heads + 8 * i;
-            const unsigned n = h[0] & 255u, m = h[1];
-            if (n < 2 || n > CE_MAX_NODES || m > CE_MAX_MUSCLES) {
-                set_error("Unsupported body for the CUDA kernel: " + std::to_string(n) + " nodes, " +
-                          std::to_string(m) + " muscles");
-                return CE_ERR_INVALID;
-            }
-            if ((n > kSmallBody) != (big != 0)) continue;
-            order.push_back((uint32_t)i);
-            c.rows = std::max(c.rows, n);
-            c.mm = std::max(c.mm, m);
+    size_t per_n[CE_MAX_NODES + 1] = {};
+    uint32_t mm_n[CE_MAX_NODES + 1] = {};
+    for (size_t i = 0; i < pack->count; i++) {
+        const uint32_t* h = pack->heads + 8 * i;
+        const unsigned n = h[0] & 255u, m = h[1];
+        if (n < 2 || n > CE_MAX_NODES || m > CE_MAX_MUSCLES) {
+            set_error("Unsupported body for the CUDA kernel: " + std::to_string(n) + " nodes, " +
+                      std::to_string(m) + " muscles");
+            return CE_ERR_INVALID;
         }
-        c.count = (uint32_t)order.size() - c.first;
+        per_n[n]++;
+        mm_n[n] = std::max(mm_n[n], m);
+    }
+    for (int big = 0; big < 2; big++) {
+        ClassPlan c{0, 0, 0, 2, 0};
+        for (unsigned n = 2; n <= CE_MAX_NODES; n++) {
+            if (per_n[n] == 0 || (n > kSmallBody) != (big != 0)) continue;
+            if (c.count == 0) c.first_n = n;
+            c.last_n = n;
+            c.count += (uint32_t)per_n[n];
+            c.rows = n;
+            c.mm = std::max(c.mm, mm_n[n]);
+        }
         if (c.count) plans.push_back(c);
     }
     return CE_OK;
@@ -227,6 +236,8 @@ extern "C" ce_status ce_open(int device, const ce_options* options, ce_engine** 
         if (s == CE_OK) s = cuda_status(cudaStreamCreateWithFlags(&sl.side, cudaStreamNonBlocking), "cudaStreamCreate");
         if (s == CE_OK)
             s = cuda_status(cudaEventCreateWithFlags(&sl.joined, cudaEventDisableTiming), "cudaEventCreate");
+        if (s == CE_OK)
+            s = cuda_status(cudaEventCreateWithFlags(&sl.bucketed, cudaEventDisableTiming), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.start), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreate(&sl.stop), "cudaEventCreate");
         if (s == CE_OK) s = cuda_status(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "cudaEventCreate");
@@ -248,8 +259,7 @@ extern "C" ce_status ce_close(ce_engine* e) {
         sl.d_muscles.release();
         sl.d_heads.release();
         sl.d_results.release();
-        sl.d_order.release();
-        sl.d_counters.release();
+        sl.d_buckets.release();
         sl.d_scratch.release();
         sl.h_upload.release();
         sl.h_results.release();
@@ -257,6 +267,7 @@ extern "C" ce_status ce_close(ce_engine* e) {
         if (sl.stop) cudaEventDestroy(sl.stop);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.joined) cudaEventDestroy(sl.joined);
+        if (sl.bucketed) cudaEventDestroy(sl.bucketed);
         if (sl.side) cudaStreamDestroy(sl.side);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
@@ -283,8 +294,8 @@ extern "C" size_t ce_allocated_bytes(ce_engine* e) {
     size_t b = e->rec_frames.bytes + e->rec_lanes.bytes + e->rec_muscles.bytes + e->rec_heads.bytes +
                e->rec_results.bytes + e->rec_counter.bytes + e->rec_scratch.bytes;
     for (const Slot& sl : e->slots) {
-        b += sl.d_lanes.bytes + sl.d_muscles.bytes + sl.d_heads.bytes + sl.d_results.bytes + sl.d_order.bytes +
-             sl.d_counters.bytes + sl.d_scratch.bytes;
+        b += sl.d_lanes.bytes + sl.d_muscles.bytes + sl.d_heads.bytes + sl.d_results.bytes + sl.d_buckets.bytes +
+             sl.d_scratch.bytes;
     }
     return b;
 }
@@ -298,8 +309,7 @@ extern "C" ce_status ce_release_idle(ce_engine* e) {
         sl.d_muscles.release();
         sl.d_heads.release();
         sl.d_results.release();
-        sl.d_order.release();
-        sl.d_counters.release();
+        sl.d_buckets.release();
         sl.d_scratch.release();
         sl.h_upload.release();
         sl.h_results.release();
@@ -340,9 +350,8 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     }
     Slot& sl = e->slots[si];
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
-    std::vector<uint32_t> order;
     std::vector<ClassPlan> plans;
-    if ((s = plan_classes(pack, order, plans)) != CE_OK) return s;
+    if ((s = plan_classes(pack, plans)) != CE_OK) return s;
     const uint32_t flags = ce_world_flags(w);
     const int rate = (int)ce::world_rate(*w);
     ce_params p;
@@ -358,11 +367,11 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
         scratch += (scratch_bytes(grids[c], plans[c].rows, plans[c].mm, false) + 255u) & ~(size_t)255u;
     }
     const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
-    const size_t order_b = order.size() * 4, res_b = pack->count * sizeof(ce_result);
+    const size_t res_b = pack->count * sizeof(ce_result);
     if ((s = sl.d_lanes.ensure(lanes_b)) || (s = sl.d_muscles.ensure(mus_b)) || (s = sl.d_heads.ensure(heads_b)) ||
-        (s = sl.d_order.ensure(std::max<size_t>(order_b, 4))) || (s = sl.d_results.ensure(res_b)) ||
-        (s = sl.d_counters.ensure(64)) || (s = sl.d_scratch.ensure(scratch)) ||
-        (s = sl.h_upload.ensure(lanes_b + mus_b + heads_b + order_b)) || (s = sl.h_results.ensure(res_b))) {
+        (s = sl.d_buckets.ensure(cek::bucket_bytes(pack->count))) || (s = sl.d_results.ensure(res_b)) ||
+        (s = sl.d_scratch.ensure(scratch)) || (s = sl.h_upload.ensure(lanes_b + mus_b + heads_b)) ||
+        (s = sl.h_results.ensure(res_b))) {
         return s;
     }
     // Stage the batch in pinned memory, then copy it up asynchronously.
@@ -370,29 +379,30 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     std::memcpy(up, pack->lanes, lanes_b);
     std::memcpy(up + lanes_b, pack->muscles, mus_b);
     std::memcpy(up + lanes_b + mus_b, pack->heads, heads_b);
-    if (order_b) std::memcpy(up + lanes_b + mus_b + heads_b, order.data(), order_b);
     cudaStream_t st = sl.stream;
     CE_TRY(cudaMemcpyAsync(sl.d_lanes.ptr, up, lanes_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     CE_TRY(cudaMemcpyAsync(sl.d_muscles.ptr, up + lanes_b, mus_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     CE_TRY(cudaMemcpyAsync(sl.d_heads.ptr, up + lanes_b + mus_b, heads_b, cudaMemcpyHostToDevice, st),
            "cudaMemcpyAsync");
-    if (order_b) {
-        CE_TRY(cudaMemcpyAsync(sl.d_order.ptr, up + lanes_b + mus_b + heads_b, order_b, cudaMemcpyHostToDevice, st),
-               "cudaMemcpyAsync");
-    }
-    CE_TRY(cudaMemsetAsync(sl.d_counters.ptr, 0, 64, st), "cudaMemsetAsync");
     CE_TRY(cudaEventRecord(sl.start, st), "cudaEventRecord");
-    CE_TRY(cudaStreamWaitEvent(sl.side, sl.start, 0), "cudaStreamWaitEvent");
+    const cek::Buckets bk = cek::bucket_layout(sl.d_buckets.ptr, pack->count);
+    CE_TRY(cek::launch_bucket(static_cast<const uint4*>(sl.d_heads.ptr), 0u, (uint32_t)pack->count, bk, st),
+           "bucketing launch");
+    CE_TRY(cudaEventRecord(sl.bucketed, st), "cudaEventRecord");
+    CE_TRY(cudaStreamWaitEvent(sl.side, sl.bucketed, 0), "cudaStreamWaitEvent");
     for (size_t c = 0; c < plans.size(); c++) {
         cek::KernelArgs a{};
         a.records = static_cast<const uint32_t*>(sl.d_lanes.ptr);
         a.muscles = static_cast<const float*>(sl.d_muscles.ptr);
         a.heads = static_cast<const uint4*>(sl.d_heads.ptr);
         a.results = static_cast<ce_result*>(sl.d_results.ptr);
-        a.counter = static_cast<uint32_t*>(sl.d_counters.ptr) + c;
+        a.counter = bk.counters + plans[c].first_n;
         a.scratch = reinterpret_cast<float4*>(static_cast<char*>(sl.d_scratch.ptr) + scratch_at[c]);
         a.frames = nullptr;
-        a.order = static_cast<const uint32_t*>(sl.d_order.ptr) + plans[c].first;
+        a.order = bk.order;
+        a.bounds = bk.bounds + plans[c].first_n;
+        a.work = bk.work + plans[c].first_n;
+        a.queues = plans[c].last_n - plans[c].first_n + 1u;
         a.count = plans[c].count;
         a.rows = plans[c].rows;
         a.mm = plans[c].mm;
@@ -484,9 +494,8 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
         set_error("ce_record: at most 64 creatures a recording");
         return CE_ERR_INVALID;
     }
-    std::vector<uint32_t> order;
     std::vector<ClassPlan> plans;
-    if ((s = plan_classes(pack, order, plans)) != CE_OK) return s;
+    if ((s = plan_classes(pack, plans)) != CE_OK) return s;
     unsigned rows = 2, mm = 0;
     for (const ClassPlan& c : plans) {
         rows = std::max(rows, c.rows);
@@ -539,12 +548,20 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     return CE_OK;
 }
 
+// The device entry's scratch: the lane slots of the grid, then the claim
+// queues of `count` creatures.
+namespace {
+size_t slots_part(ce_engine* e, uint32_t world_flags, uint32_t rate, uint32_t max_nodes, uint32_t max_muscles) {
+    const unsigned grid = grid_for(e, max_nodes, max_muscles, world_flags, false, (int)rate, (size_t)1 << 30);
+    return (scratch_bytes(grid, max_nodes, max_muscles, false) + 255u) & ~(size_t)255u;
+}
+}  // namespace
+
 extern "C" size_t ce_advance_scratch_bytes(ce_engine* e, uint32_t world_flags, uint32_t rate, uint32_t max_nodes,
-                                           uint32_t max_muscles) {
+                                           uint32_t max_muscles, uint32_t count) {
     if (!e || max_nodes < 2 || max_nodes > CE_MAX_NODES || max_muscles > CE_MAX_MUSCLES) return 0;
     if (rate != 60 && rate != 120) return 0;
-    const unsigned grid = grid_for(e, max_nodes, max_muscles, world_flags, false, (int)rate, (size_t)1 << 30);
-    return scratch_bytes(grid, max_nodes, max_muscles, false);
+    return slots_part(e, world_flags, rate, max_nodes, max_muscles) + cek::bucket_bytes(count);
 }
 
 extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, const float* muscles,
@@ -562,22 +579,29 @@ extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, co
     }
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
     const unsigned grid = grid_for(e, max_nodes, max_muscles, world_flags, false, (int)rate, params->count);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const cek::Buckets bk = cek::bucket_layout(
+        static_cast<char*>(scratch) + slots_part(e, world_flags, rate, max_nodes, max_muscles), params->count);
+    CE_TRY(cek::launch_bucket(reinterpret_cast<const uint4*>(heads), params->base, params->count, bk, st),
+           "bucketing launch");
     cek::KernelArgs a{};
     a.records = records;
     a.muscles = muscles;
     a.heads = reinterpret_cast<const uint4*>(heads);
     a.results = results;
-    a.counter = counter;
+    a.counter = bk.counters;
     a.scratch = static_cast<float4*>(scratch);
     a.frames = nullptr;
-    a.order = nullptr;
+    a.order = bk.order;
+    a.bounds = bk.bounds;
+    a.work = bk.work;
+    a.queues = cek::kQueues;
     a.count = params->count;
     a.rows = max_nodes;
     a.mm = max_muscles;
     a.frames_per_creature = 0;
     a.chunk_k = e->chunk_k;
-    cek::LaunchSpec ls{max_nodes, max_muscles, world_flags, false, (int)rate, grid, cek::kBlock,
-                       static_cast<cudaStream_t>(stream)};
+    cek::LaunchSpec ls{max_nodes, max_muscles, world_flags, false, (int)rate, grid, cek::kBlock, st};
     CE_TRY(cek::launch_advance(ls, a, *params), "advance launch");
     return CE_OK;
 }

@@ -31,21 +31,50 @@ inline size_t smem_bytes(unsigned rows, unsigned mm, unsigned block) {
     return (size_t)block * (rows * 24u + (mm > 0 ? mm : 1u) * 8u);
 }
 
+// Claim queues. A launch with queues takes its creatures from one queue per
+// node count: queue q holds order[bounds[q] .. bounds[q + 1]), claimed
+// through counter[q], and work[q] is the estimated work of the queues below
+// q. Inside a queue the creatures keep the packed order, whose muscle count
+// ascends, so the lanes of a warp hold bodies of the same node count and
+// nearly the same muscle count and its loops run to nearly the same length.
+constexpr unsigned kQueues = CE_MAX_NODES + 1u;  // node counts 0..32
+constexpr unsigned kBucketTile = 4096u;          // creatures a block buckets
+
 struct KernelArgs {
     const uint32_t* records;
     const float* muscles;
     const uint4* heads;
     ce_result* results;
-    uint32_t* counter;
+    uint32_t* counter;             // one claim counter a queue (one for no queues), zeroed
     float4* scratch;               // slots: warps of the grid x lines x 32 lanes
     float2* frames;                // RECORD: frames of each recorded creature
     const uint32_t* order;         // packed positions of this launch's creatures
+    const uint32_t* bounds;        // queues + 1 positions of the order list
+    const unsigned long long* work;  // queues + 1 prefix sums of estimated work
+    uint32_t queues;               // 0: one queue, positions 0 .. count - 1
     uint32_t count;                // creatures of this launch
     uint32_t rows;                 // node rows: most nodes of a body of this launch
     uint32_t mm;                   // most muscles of a body of this launch
     uint32_t frames_per_creature;  // RECORD: frames of one recording
     uint32_t chunk_k;              // claims shrink to 1 / chunk_k of the rest per warp
 };
+
+// The device arrays that bucketing writes for `count` creatures, carved from
+// one area of bucket_bytes(count) bytes.
+struct Buckets {
+    uint32_t* order;            // count packed positions, node count by node count
+    uint32_t* hist;             // kQueues x tiles: creatures of each node count per tile
+    uint32_t* bounds;           // kQueues + 1
+    unsigned long long* work;   // kQueues + 1
+    unsigned long long* bins;   // kQueues: estimated work of each node count
+    uint32_t* counters;         // kQueues, zeroed by the bucketing
+    uint32_t tiles;
+};
+size_t bucket_bytes(size_t count);
+Buckets bucket_layout(void* area, size_t count);
+// Buckets creatures base .. base + count - 1 of a packed batch by node count
+// (three kernels on `stream`); the heads give the node and muscle counts.
+cudaError_t launch_bucket(const uint4* heads, uint32_t base, uint32_t count, const Buckets& b, cudaStream_t stream);
 
 struct LaunchSpec {
     unsigned rows;   // node rows of the tables (most nodes of a body)

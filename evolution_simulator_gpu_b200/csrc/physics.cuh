@@ -254,6 +254,18 @@ struct Lines {
     __device__ __forceinline__ float& word(unsigned L, unsigned k) const {
         return reinterpret_cast<float*>(&base[L * 32u])[k];
     }
+    // Lines touched once a step (muscle rhythm and state, the lane lines) go
+    // through the evict-first cache operator (ld/st.global.cs), so the lines
+    // that every substep reads keep their place in L2: the slots of all
+    // resident lanes together are about as large as L2.
+    __device__ __forceinline__ float4 get_cold(unsigned L) const { return __ldcs(&base[L * 32u]); }
+    __device__ __forceinline__ void put_cold(unsigned L, float4 v) const { __stcs(&base[L * 32u], v); }
+    __device__ __forceinline__ float word_cold(unsigned L, unsigned k) const {
+        return __ldcs(reinterpret_cast<const float*>(&base[L * 32u]) + k);
+    }
+    __device__ __forceinline__ void set_cold(unsigned L, unsigned k, float v) const {
+        __stcs(reinterpret_cast<float*>(&base[L * 32u]) + k, v);
+    }
 };
 
 // Where each kind of line starts in a slot of a class with NS node rows and

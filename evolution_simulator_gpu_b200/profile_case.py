@@ -28,6 +28,7 @@ def main() -> None:
     ap.add_argument("--creatures", type=int, default=300_000)
     ap.add_argument("--seconds", type=float, default=1.0)
     ap.add_argument("--reference", action="store_true")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="resident blocks per SM (0: the engine's choice)")
     args = ap.parse_args()
     import evolution_simulator_gpu_b200 as ce
     from evolution_simulator_gpu_b200.configs import WORKLOADS
@@ -35,9 +36,10 @@ def main() -> None:
     world = w.world(duration=args.seconds)
     pop = ce.generate(w.spec, args.creatures)
     wave = ce.pack(pop, world)
-    with ce.Engine(0) as eng:
+    with ce.Engine(0, ctas_per_sm=args.ctas_per_sm) as eng:
         mine, busy = eng.run(wave, world)
-    out = {"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds, "engine_s": busy,
+    out = {"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds,
+           "ctas_per_sm": args.ctas_per_sm, "engine_s": busy,
            "creature_substeps": ce.creature_substeps(mine, world),
            "record_bytes": int(wave.lanes.nbytes + wave.muscles.nbytes + wave.heads.nbytes)}
     if args.reference:

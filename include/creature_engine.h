@@ -291,10 +291,13 @@ ce_status ce_record(ce_engine* engine, const ce_wave_pack* pack, const ce_world*
  * on `stream` (a cudaStream_t, NULL for the legacy stream). `rate` is the
  * step rate the reference compiles into its kernel (60 or 120). Bodies must
  * have at most `max_nodes` nodes and `max_muscles` muscles. `scratch` is a
- * device buffer of at least ce_advance_scratch_bytes() bytes, `counter`
- * a device word set to 0 before the call. Asynchronous. */
+ * device buffer of at least ce_advance_scratch_bytes(..., params->count)
+ * bytes: the lane slots, and the claim queues that the call first builds
+ * by bucketing the creatures by node count (with their claim counters,
+ * zeroed by the call). `counter` is kept from the reference's kernel
+ * arguments; this entry neither reads nor writes it. Asynchronous. */
 size_t ce_advance_scratch_bytes(ce_engine* engine, uint32_t world_flags, uint32_t rate,
-                                uint32_t max_nodes, uint32_t max_muscles);
+                                uint32_t max_nodes, uint32_t max_muscles, uint32_t count);
 ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const float* muscles,
                             const uint32_t* heads, ce_result* results, uint32_t* counter,
                             void* scratch, const ce_params* params, uint32_t world_flags,

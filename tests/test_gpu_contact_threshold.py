@@ -107,7 +107,7 @@ def test_contact_threshold_matches_reference():
         d_h = torch.from_numpy(wave.heads.view(np.int32).reshape(-1)).to(dev)
         d_r = torch.zeros(len(wave) * 19, device=dev)
         d_c = torch.zeros(16, dtype=torch.int32, device=dev)
-        d_s = torch.empty(eng.scratch_bytes(EFFECTS, 60, 3, 0), dtype=torch.uint8, device=dev)
+        d_s = torch.empty(eng.scratch_bytes(EFFECTS, 60, 3, 0, len(wave)), dtype=torch.uint8, device=dev)
         p.count = len(wave)
         eng.advance_device(d_l.data_ptr(), d_m.data_ptr(), d_h.data_ptr(), d_r.data_ptr(), d_c.data_ptr(),
                            d_s.data_ptr(), p, EFFECTS, 60, 3, 0, torch.cuda.current_stream(dev).cuda_stream)

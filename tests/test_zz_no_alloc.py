@@ -40,7 +40,7 @@ def test_no_alloc_entry_matches_the_device_entry_twice():
     with ce.Engine(0) as eng:
         d_res = torch.zeros(len(wave) * 19, dtype=torch.float32, device=dev)
         d_counter = torch.zeros(16, dtype=torch.int32, device=dev)
-        d_scratch = torch.empty(eng.scratch_bytes(flags, rate, wave.max_nodes, wave.max_muscles), dtype=torch.uint8,
+        d_scratch = torch.empty(eng.scratch_bytes(flags, rate, wave.max_nodes, wave.max_muscles, len(wave)), dtype=torch.uint8,
                                 device=dev)
         eng.advance_device(d_lanes.data_ptr(), d_muscles.data_ptr(), d_heads.data_ptr(), d_res.data_ptr(),
                            d_counter.data_ptr(), d_scratch.data_ptr(), params, flags, rate, wave.max_nodes,
