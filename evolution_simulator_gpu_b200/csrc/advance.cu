@@ -68,7 +68,7 @@ struct Trial {
             const uint32_t* q = rec + i * CE_NODE_WORDS;
             const float m = __uint_as_float(__ldcs(q + 0));
             L.put(S.node + i, make_float4(m, 1.0f / m, __uint_as_float(__ldcs(q + 1)), __uint_as_float(__ldcs(q + 2))));
-            b.t.at(i) = make_float4(__uint_as_float(__ldcs(q + 3)), __uint_as_float(__ldcs(q + 4)), 0.0f, 0.0f);
+            b.t.set_at(i, make_float4(__uint_as_float(__ldcs(q + 3)), __uint_as_float(__ldcs(q + 4)), 0.0f, 0.0f));
             r.feet |= (__ldcs(q + 5) & 1u) << i;
             if (RECORD) {
                 L.put(S.rec_force + i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
@@ -469,9 +469,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const Kerne
     extern __shared__ float4 smem[];
     using T = Trial<W, RECORD, RATE>;
     const unsigned threads = blockDim.x;
-    float2* fp_base = reinterpret_cast<float2*>(smem + a.rows * threads);
-    const NodeTables tab{smem + threadIdx.x, fp_base + threadIdx.x, fp_base + a.rows * threads + threadIdx.x,
-                         threads};
+    // Tables of rows x threads entries: positions, velocities, forces, then
+    // the muscles' (energy, demand) pairs.
+    float2* const tables = reinterpret_cast<float2*>(smem) + threadIdx.x;
+    const size_t table = (size_t)a.rows * threads;
+    const NodeTables tab{tables, tables + table, tables + 2u * table, tables + 3u * table, threads};
     const SlotLayout S = SlotLayout::make(a.rows, a.mm, RECORD);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = (blockIdx.x * threads + threadIdx.x) >> 5u;

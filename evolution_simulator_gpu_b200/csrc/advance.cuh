@@ -364,7 +364,7 @@ struct Creature {
             t.f(i) = make_float2(s.x, s.y);
             s.x += C::h * s.z;
             s.y += C::h * s.w;
-            t.at(i) = s;
+            t.set_at(i, s);
         }
         solve_bones();
         solve_joints();

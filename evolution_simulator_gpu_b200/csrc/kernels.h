@@ -24,9 +24,9 @@ constexpr uint32_t kWorldEffects = CE_FLAG_GROUND | CE_FLAG_TERRAIN | CE_FLAG_SL
 constexpr uint32_t kWorldEffectsQuake = kWorldEffects | CE_FLAG_QUAKE;
 constexpr uint32_t kWorldAll = 0xfffu;
 
-// Shared memory of a block: the position/velocity table (16 bytes) and the
-// force table (8 bytes) for `rows` node rows of every thread, and the
-// (energy store, demand) pair of `mm` muscles of every thread.
+// Shared memory of a block: the position, velocity and force tables (8 bytes
+// each) for `rows` node rows of every thread, and the (energy store, demand)
+// pair of `mm` muscles of every thread.
 inline size_t smem_bytes(unsigned rows, unsigned mm, unsigned block) {
     return (size_t)block * (rows * 24u + (mm > 0 ? mm : 1u) * 8u);
 }

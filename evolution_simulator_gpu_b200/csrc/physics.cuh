@@ -7,10 +7,10 @@
 // same rounding and the same fused multiply-adds under nvcc's
 // -fmad=true -prec-div=false -prec-sqrt=false. The data layout is this
 // engine's own:
-//   * node state sits in two shared-memory tables, one column per lane:
-//     `pv` holds (x, y, vx, vy) per node and `fp` the force / previous
-//     position pair, so a pass that needs a node's position and velocity
-//     makes one 16-byte load;
+//   * node state sits in shared-memory tables, one column per lane and
+//     8 bytes an entry: positions, velocities, and the force / previous
+//     position pair, so every access of a warp to one table is free of bank
+//     conflicts;
 //   * a creature's constants sit in 16-byte "lines" of a per-lane slot in
 //     global memory, laid out lane-major (line L of lane l at
 //     slot + (L * 32 + l) * 16), so the 32 lanes of a warp read a line as one
@@ -230,19 +230,26 @@ __device__ __forceinline__ float ice_at(float x) {
 // Node state of the lanes of a block in shared memory. Row i of a table
 // holds node i of every lane, so a warp reads a row without bank conflicts
 // whatever node each lane asks for.
+// Position and velocity have tables of their own: a lane's 8-byte entries
+// then lie 8 bytes apart across the lanes, so a warp reading positions only
+// (or velocities only) meets no bank twice.
 struct NodeTables {
-    float4* pv;  // (x, y, vx, vy)
+    float2* p;   // (x, y)
+    float2* v;   // (vx, vy)
     float2* fp;  // muscle force, then the position at the start of the substep
     float2* ms;  // per muscle: (energy store, demand of the step)
     unsigned stride;  // threads of the block
-    __device__ __forceinline__ float4& at(unsigned i) const { return pv[i * stride]; }
+    __device__ __forceinline__ float4 at(unsigned i) const {
+        const float2 q = p[i * stride], u = v[i * stride];
+        return make_float4(q.x, q.y, u.x, u.y);
+    }
+    __device__ __forceinline__ void set_at(unsigned i, const float4& s) const {
+        p[i * stride] = make_float2(s.x, s.y);
+        v[i * stride] = make_float2(s.z, s.w);
+    }
     __device__ __forceinline__ float2& f(unsigned i) const { return fp[i * stride]; }
-    __device__ __forceinline__ float2& pos(unsigned i) const {
-        return *reinterpret_cast<float2*>(&pv[i * stride].x);
-    }
-    __device__ __forceinline__ float2& vel(unsigned i) const {
-        return *reinterpret_cast<float2*>(&pv[i * stride].z);
-    }
+    __device__ __forceinline__ float2& pos(unsigned i) const { return p[i * stride]; }
+    __device__ __forceinline__ float2& vel(unsigned i) const { return v[i * stride]; }
     __device__ __forceinline__ float2& muscle(unsigned k) const { return ms[k * stride]; }
 };
 
