@@ -83,17 +83,24 @@ struct Creature {
                k.w_far * (k.g_far.x * k.g_far.x + k.g_far.y * k.g_far.y) +
                k.w_hub * (k.g_hub.x * k.g_hub.x + k.g_hub.y * k.g_hub.y);
     }
+    // Each node as one 8-byte load and store: tip, far, then hub.
     template <bool VEL>
     __device__ __forceinline__ void joint_push(const Joint& k, float lambda) const {
         float2& tip = VEL ? t.vel(k.tip) : t.pos(k.tip);
+        float2 e = tip;
+        e.x += k.w_tip * lambda * k.g_tip.x;
+        e.y += k.w_tip * lambda * k.g_tip.y;
+        tip = e;
         float2& far = VEL ? t.vel(k.far) : t.pos(k.far);
+        e = far;
+        e.x += k.w_far * lambda * k.g_far.x;
+        e.y += k.w_far * lambda * k.g_far.y;
+        far = e;
         float2& hub = VEL ? t.vel(k.hub) : t.pos(k.hub);
-        tip.x += k.w_tip * lambda * k.g_tip.x;
-        tip.y += k.w_tip * lambda * k.g_tip.y;
-        far.x += k.w_far * lambda * k.g_far.x;
-        far.y += k.w_far * lambda * k.g_far.y;
-        hub.x += k.w_hub * lambda * k.g_hub.x;
-        hub.y += k.w_hub * lambda * k.g_hub.y;
+        e = hub;
+        e.x += k.w_hub * lambda * k.g_hub.x;
+        e.y += k.w_hub * lambda * k.g_hub.y;
+        hub = e;
     }
 
     // Each muscle's demand for the step that starts at t_now
@@ -155,14 +162,24 @@ struct Creature {
                 L.word(S.rec_pull + k / 4u, k % 4u) = pull;
             }
             const float fx = ex * pull, fy = ey * pull;
-            t.f(a0).x += fx * (1.0f - anchor_a);
-            t.f(a0).y += fy * (1.0f - anchor_a);
-            t.f(a1).x += fx * anchor_a;
-            t.f(a1).y += fy * anchor_a;
-            t.f(b0).x -= fx * (1.0f - anchor_b);
-            t.f(b0).y -= fy * (1.0f - anchor_b);
-            t.f(b1).x -= fx * anchor_b;
-            t.f(b1).y -= fy * anchor_b;
+            // One 8-byte load and store per node, in the order a0, a1, b0,
+            // b1 (two of them may be the same node).
+            float2 g = t.f(a0);
+            g.x += fx * (1.0f - anchor_a);
+            g.y += fy * (1.0f - anchor_a);
+            t.f(a0) = g;
+            g = t.f(a1);
+            g.x += fx * anchor_a;
+            g.y += fy * anchor_a;
+            t.f(a1) = g;
+            g = t.f(b0);
+            g.x -= fx * (1.0f - anchor_b);
+            g.y -= fy * (1.0f - anchor_b);
+            t.f(b0) = g;
+            g = t.f(b1);
+            g.x -= fx * anchor_b;
+            g.y -= fy * anchor_b;
+            t.f(b1) = g;
         }
     }
 
@@ -224,10 +241,8 @@ struct Creature {
                 dfy -= sy * k_water + ly * k_water * kWaterAlong;
             }
             const float s0 = bb.z, s1 = bb.w;
-            t.vel(i0).x += s0 * dfx;
-            t.vel(i0).y += s0 * dfy;
-            t.vel(i1).x += s1 * dfx;
-            t.vel(i1).y += s1 * dfy;
+            t.vel(i0) = make_float2(v0.x + s0 * dfx, v0.y + s0 * dfy);
+            t.vel(i1) = make_float2(v1.x + s1 * dfx, v1.y + s1 * dfy);
         }
     }
 
@@ -244,10 +259,8 @@ struct Creature {
             const float len = fmaxf(sqrtf(dx * dx + dy * dy), 1e-9f);
             const float w0 = ba.z, w1 = ba.w;
             const float s = (len - ba.y) / ((w0 + w1) * len);
-            t.pos(i0).x += w0 * s * dx;
-            t.pos(i0).y += w0 * s * dy;
-            t.pos(i1).x -= w1 * s * dx;
-            t.pos(i1).y -= w1 * s * dy;
+            t.pos(i0) = make_float2(p0.x + w0 * s * dx, p0.y + w0 * s * dy);
+            t.pos(i1) = make_float2(p1.x - w1 * s * dx, p1.y - w1 * s * dy);
         }
     }
 
@@ -281,14 +294,16 @@ struct Creature {
     }
 
     // Ground contact and friction of node i (shaders/creature.cu:640-679).
-    __device__ __forceinline__ void solve_ground(unsigned i, const float4& nr) const {
+    // `q` is the node's position (updated and stored when it touches) and
+    // `f0` its position at the start of the substep.
+    __device__ __forceinline__ void solve_ground(unsigned i, const float4& nr, float2& q, const float2& f0) const {
         if (!w.has(CE_FLAG_GROUND)) {
             return;
         }
-        const float2 g = ground(w, t.pos(i).x, r.amp, r.qphase, p);
+        const float2 g = ground(w, q.x, r.amp, r.qphase, p);
         const float secant = sqrtf(1.0f + g.y * g.y);
         const float nx = -g.y / secant, ny = 1.0f / secant;
-        const float dry = (t.pos(i).y - g.x) / secant - nr.z;
+        const float dry = (q.y - g.x) / secant - nr.z;
         float depth, mu;
         if (w.has(CE_FLAG_MUD)) {
             depth = -(dry + p.mud);
@@ -302,17 +317,17 @@ struct Creature {
             return;
         }
         if (w.has(CE_FLAG_ICE)) {
-            mu *= 1.0f - p.patches * ice_at(t.pos(i).x);
+            mu *= 1.0f - p.patches * ice_at(q.x);
         }
-        t.pos(i).x += nx * depth;
-        t.pos(i).y += ny * depth;
+        q.x += nx * depth;
+        q.y += ny * depth;
         const float tx = ny, ty = -nx;
-        const float2 q = t.pos(i), f0 = t.f(i);
         const float slide = (q.x - f0.x) * tx + (q.y - f0.y) * ty;
         const float budget = mu * depth;
         const float back = fabsf(slide) <= budget ? slide : copysignf(budget, slide);
-        t.pos(i).x -= tx * back;
-        t.pos(i).y -= ty * back;
+        q.x -= tx * back;
+        q.y -= ty * back;
+        t.pos(i) = q;
         if (RECORD) {
             float4 fl = L.get(S.rec_force + i);
             fl.x += nr.x * depth * C::inv_h * C::inv_h;
@@ -372,8 +387,9 @@ struct Creature {
         for (unsigned i = 0u; i < r.nodes; i++) {
             const float4 nr = nn;
             nn = L.get(S.node + i + 1u);
-            solve_ground(i, nr);
-            const float2 q = t.pos(i), f0 = t.f(i);
+            float2 q = t.pos(i);
+            const float2 f0 = t.f(i);
+            solve_ground(i, nr, q, f0);
             t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
         }
         damp_joints();
