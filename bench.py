@@ -167,11 +167,16 @@ def op_counts() -> dict:
     return json.loads(path.read_text()) if path.exists() else {}
 
 
-def traffic_per_substep():
+def traffic_model():
+    """(bytes per creature, bytes per creature-substep) of DRAM traffic of the
+    creature kernel, from two ncu captures (profiles/traffic.json)."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
         return None
-    return json.loads(path.read_text()).get(WORKLOAD, {}).get("dram_bytes_per_substep")
+    t = json.loads(path.read_text()).get(WORKLOAD, {})
+    if "dram_bytes_per_substep" not in t:
+        return None
+    return t.get("dram_bytes_per_creature", 0.0), t["dram_bytes_per_substep"]
 
 
 # ---------------------------------------------------------------- CPU baseline
@@ -290,10 +295,11 @@ def run_engine(args):
         flops_per = counts.get("flops_per_substep")
         peak = ce.measure_fp32(local)
         achieved = flops_per * units / (per_launch_ms / 1e3) / 1e12 if flops_per else None
-        tps = traffic_per_substep()
+        tm = traffic_model()
         roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak if achieved else None,
-                    "traffic": tps * units if tps else None,
+                    "traffic": tm[0] * len(wave) + tm[1] * units if tm else None,
+                    "traffic_unit": "bytes per launch (ncu capture scaled by creatures and substeps)",
                     "peak_source": "measured: FP32 multiply-add calibration kernel (ce_measure_fp32) on this GPU",
                     "numerator": f"{flops_per:.0f} algorithmic FP32 operations per creature-substep "
                                  "(oracle op count, profiles/op_counts.json) x creature-substeps of the launch"
