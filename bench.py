@@ -34,7 +34,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "creature-substeps/s at 3M creatures x 20 s"
+METRIC = "creature-substeps/s at 3M creatures x 20 s; adjoint grads/s vs plain-path FD"
 UNIT = "creature-substeps/s"
 WORKLOAD = "game"
 # Kernels of one device-entry call besides the creature kernel: the node-count
@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--creatures", type=int, default=3_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-adjoint", action="store_true", help="leave out the gradient measurement")
     return ap.parse_args()
 
 
@@ -216,6 +217,44 @@ def cpu_baseline(wave, world, budget_s: float) -> dict:
                       f"{done:.3g} creature-substeps in {secs:.1f} s"}
 
 
+# ---------------------------------------------------------------- gradients
+ADJOINT_TEXT = ("65,536 seeded synthetic creatures (seed 3), 4-12 nodes, 4-20 muscles, flat grippy calm world, "
+                "20 s trials, FP32, checkpoints every 256 substeps; gradient = d fitness / d (short, long, strength, "
+                "on time, off time of every muscle, friction of every node)")
+
+
+def gradient_workload():
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS["gradients"]
+    world = w.world()
+    pop = ce.generate(w.spec, w.creatures)
+    wave = ce.pack(pop, world)
+    params = 5 * wave.heads[:, 1].astype(np.int64).sum() + (wave.heads[:, 0] & 255).astype(np.int64).sum()
+    return world, pop, wave, float(params) / len(wave)
+
+
+def adjoint_bench(eng) -> dict:
+    """Full gradients per second of the adjoint (ce_forward + ce_backward,
+    GPU time) against central finite differences on the plain kernel (2
+    forward trials a parameter, GPU time of the plain submission)."""
+    world, pop, wave, params = gradient_workload()
+    eng.run(wave, world)
+    _, plain_s = eng.run(wave, world)
+    with eng.forward(wave, world) as tape:
+        tape.backward()
+    with eng.forward(wave, world) as tape:
+        tape.backward()
+        forward_s, backward_s = tape.seconds
+    adjoint = len(wave) / (forward_s + backward_s)
+    fd = len(wave) / (plain_s * 2.0 * params)
+    return {"workload": ADJOINT_TEXT, "unit": "gradients/s", "value": adjoint, "fd_value": fd,
+            "speedup_vs_fd": adjoint / fd, "params_per_creature": params, "forward_s": forward_s,
+            "backward_s": backward_s, "plain_s": plain_s, "creatures": len(wave),
+            "timing": "CUDA events around the kernels of one batch (forward with checkpoints, backward; "
+                      "plain submission)"}
+
+
 # ---------------------------------------------------------------- engine arm
 def run_engine(args):
     world_size, rank, local = dist_setup(args.gpus)
@@ -305,6 +344,7 @@ def run_engine(args):
                                  "(oracle op count, profiles/op_counts.json) x creature-substeps of the launch"
                     if flops_per else None}
         cpu = cpu_baseline(wave, world, args.cpu_seconds)
+        adjoint = adjoint_bench(eng) if not args.no_adjoint else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -318,7 +358,7 @@ def run_engine(args):
                     "seconds_per_step": e2e_s / args.steps, "timing": "host wall clock around ce_submit+ce_poll",
                     "results_equal_device_path": same},
             "gpu_launches": (BUCKET_KERNELS + 1) * args.steps, "gpu_launches_e2e": e2e_launches,
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -367,6 +407,14 @@ def run_reference(args):
                    "what": "the reference's own kernel (shaders/creature.cu) built for sm_100a with its NVRTC "
                            "options, launched with its engine's wave and grid rule, CUDA-event time of one "
                            "generation", "seconds": ms / 1e3}
+        gworld, _, gwave, gparams = gradient_workload()
+        gkern = RefKernel(ce.world_flags(gworld), gworld.rate or 60)
+        gkern.run(gwave.take(np.arange(4096)), ce.make_params(gworld))
+        _, gms = gkern.run(gwave, ce.make_params(gworld))
+        ref_gpu["fd_gradients"] = {"unit": "gradients/s", "workload": ADJOINT_TEXT,
+                                   "value": len(gwave) / (gms / 1e3 * 2.0 * gparams),
+                                   "what": "central finite differences on the reference's kernel: 2 trials a "
+                                           "parameter (the reference has no gradients)"}
     except Exception as exc:  # the reference kernel needs a GPU
         ref_gpu = {"unavailable": str(exc).splitlines()[0]}
     sample = (f"{tot_count} creatures of the generation (chunks spread over the packed order), "

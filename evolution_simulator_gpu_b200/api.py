@@ -175,6 +175,16 @@ def _bind(lib: C.CDLL) -> None:
         "ce_noalloc_scratch_bytes": (C.c_size_t, []),
         "ce_to_metrics_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
+        "ce_forward": (C.c_int, [C.c_void_p, P(WavePackC), P(World), C.c_uint32, P(C.c_void_p)]),
+        "ce_tape_results": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+        "ce_tape_grad_floats": (C.c_uint32, [C.c_void_p]),
+        "ce_tape_shape": (C.c_int, [C.c_void_p, P(C.c_uint32), P(C.c_uint32)]),
+        "ce_tape_seconds": (C.c_int, [C.c_void_p, P(C.c_double), P(C.c_double)]),
+        "ce_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+        "ce_tape_free": (C.c_int, [C.c_void_p]),
+        "ce_tape_checkpoints": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(C.c_uint32)]),
+        "ce_gene_gradients": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_void_p, C.c_void_p,
+                                        C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -198,7 +208,8 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
             "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
-            "ce_noalloc_scratch_bytes"]
+            "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
+            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints"]
 
 
 def _check(status: int, what: str) -> None:
@@ -524,6 +535,10 @@ class Engine:
             if got[0] == t:
                 return got[1], got[2]
 
+    def forward(self, wave: WavePack, world: World, checkpoint_every: int = 256) -> "Tape":
+        """The batch's trials kept for gradients (ce_forward); see Tape."""
+        return forward(self, wave, world, checkpoint_every)
+
     def record(self, wave: WavePack, world: World):
         """Every frame of each creature of `wave` (at most 64): an array
         [creature, frame, slot, 2] in the reference's frame layout
@@ -548,6 +563,115 @@ class Engine:
         _check(lib().ce_advance_device(self.handle, records, muscles, heads, results, counter, scratch,
                                        C.byref(params), flags, rate, max_nodes, max_muscles, stream or None),
                "ce_advance_device")
+
+
+# ---------------------------------------------------------------- gradients
+GRAD_MUSCLE_FIELDS = ["amplitude", "hill", "cap", "inv_capacity", "phase", "duty", "inv_duty", "inv_complement",
+                      "stiffness"]
+GENE_MUSCLE_FIELDS = ["short", "long", "strength", "t_on", "t_off"]
+
+
+class Tape:
+    """A forward run kept for its backward pass, shaped like an autograd
+    function: `Engine.forward` saves (checkpoints every 256 substeps),
+    `backward` consumes. Calm world only."""
+
+    def __init__(self, handle: C.c_void_p, count: int):
+        self._h = handle
+        self.count = count
+
+    def _handle(self) -> C.c_void_p:
+        if not self._h:
+            raise EngineError(CE_ERR_INVALID, "the tape is freed")
+        return self._h
+
+    @property
+    def results(self) -> np.ndarray:
+        out = np.zeros(self.count, RESULT_DTYPE)
+        _check(lib().ce_tape_results(self._handle(), _ptr(out), self.count), "ce_tape_results")
+        return out
+
+    @property
+    def shape(self):
+        """(node rows, muscle slots) of the gradient records."""
+        rows, mm = C.c_uint32(), C.c_uint32()
+        _check(lib().ce_tape_shape(self._handle(), C.byref(rows), C.byref(mm)), "ce_tape_shape")
+        return rows.value, mm.value
+
+    @property
+    def seconds(self):
+        """GPU seconds of the forward run and of the last backward pass."""
+        f, b = C.c_double(), C.c_double()
+        _check(lib().ce_tape_seconds(self._handle(), C.byref(f), C.byref(b)), "ce_tape_seconds")
+        return f.value, b.value
+
+    def backward(self, dl_dfitness=None) -> np.ndarray:
+        """d(sum_c dl_dfitness[c] fitness_c) / d(record fields), one row per
+        creature in packed order: 9 floats a muscle slot (GRAD_MUSCLE_FIELDS),
+        then per node row its friction, then its mass, then its start
+        position as (x, y) pairs."""
+        per = int(lib().ce_tape_grad_floats(self._handle()))
+        out = np.zeros((self.count, per), np.float32)
+        w = None if dl_dfitness is None else np.ascontiguousarray(dl_dfitness, np.float32)
+        if w is not None and len(w) != self.count:
+            raise ValueError("one weight a creature")
+        _check(lib().ce_backward(self._handle(), _ptr(w), _ptr(out), out.size), "ce_backward")
+        return out
+
+    def checkpoints(self, steps: int) -> np.ndarray:
+        """The forward run's checkpoints [creature, checkpoint, rows x 4 +
+        muscle slots] (a trial of `steps` steps has ceil(steps / 16)):
+        positions and velocities as (x, y) pairs, then energy stores, every
+        16 steps."""
+        rows, mm = self.shape
+        n_ck = (steps + 15) // 16
+        out = np.zeros((self.count, n_ck, 4 * rows + mm), np.float32)
+        per = C.c_uint32()
+        _check(lib().ce_tape_checkpoints(self._handle(), _ptr(out), out.size, C.byref(per)), "ce_tape_checkpoints")
+        if per.value != n_ck:
+            raise ValueError(f"the tape holds {per.value} checkpoints a creature, not {n_ck}")
+        return out
+
+    def free(self) -> None:
+        if self._h:
+            lib().ce_tape_free(self._h)
+            self._h = None
+
+    def __enter__(self) -> "Tape":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def forward(engine: "Engine", wave: WavePack, world: World, checkpoint_every: int = 256) -> Tape:
+    h = C.c_void_p()
+    wc = wave.c()
+    _check(lib().ce_forward(engine.handle, C.byref(wc), C.byref(world), checkpoint_every, C.byref(h)),
+           "ce_forward")
+    return Tape(h, len(wave))
+
+
+def gene_gradients(pop: Population, wave: WavePack, world: World, grads: np.ndarray, shape, indices=None):
+    """Gene gradients from record gradients (Tape.backward): an (muscle genes,
+    5) array of d/d (GENE_MUSCLE_FIELDS) and a (node genes,) array of
+    d/d friction, float64; creatures outside the batch stay 0. `indices` are
+    those the batch was packed with."""
+    rows, mm = shape
+    pc = pop.c()
+    idx = None if indices is None else np.ascontiguousarray(indices, np.uint32)
+    g = np.ascontiguousarray(grads, np.float32)
+    mg = np.zeros((len(pop.muscles), 5), np.float64)
+    ng = np.zeros(len(pop.nodes), np.float64)
+    _check(lib().ce_gene_gradients(C.byref(pc), _ptr(idx), len(wave), C.byref(world), _ptr(wave.slots), _ptr(g),
+                                   rows, mm, _ptr(mg), _ptr(ng)), "ce_gene_gradients")
+    return mg, ng
 
 
 def evaluate(engine: Engine, pop: Population, world: World, indices=None) -> np.ndarray:

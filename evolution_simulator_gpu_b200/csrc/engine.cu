@@ -605,3 +605,248 @@ extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, co
     CE_TRY(cek::launch_advance(ls, a, *params), "advance launch");
     return CE_OK;
 }
+
+// ------------------------------------------------------------- gradients
+// A forward run kept for its backward pass (shaped like an autograd
+// function: ce_forward saves, ce_backward consumes). It owns its device
+// buffers and stream; one forward, then any number of backward passes.
+struct ce_tape {
+    ce_engine* engine = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    size_t count = 0;
+    unsigned rows = 2, mm = 0, ckpts = 0, grid = 1;
+    int rate = 60;
+    ce_params params{};
+    DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_buckets, d_ckpt, d_ends, d_scratch, d_tape, d_grads,
+        d_weights;
+    std::vector<ce_result> results;
+    double forward_seconds = 0.0, backward_seconds = 0.0;
+};
+
+namespace {
+
+ce_status tape_time(ce_tape* t, double* seconds) {
+    CE_TRY(cudaEventSynchronize(t->stop), "gradient kernels");
+    float ms = 0.0f;
+    CE_TRY(cudaEventElapsedTime(&ms, t->start, t->stop), "cudaEventElapsedTime");
+    *seconds = ms * 1e-3;
+    return CE_OK;
+}
+
+cek::KernelArgs tape_args(ce_tape* t, const cek::Buckets& bk) {
+    cek::KernelArgs a{};
+    a.records = static_cast<const uint32_t*>(t->d_lanes.ptr);
+    a.muscles = static_cast<const float*>(t->d_muscles.ptr);
+    a.heads = static_cast<const uint4*>(t->d_heads.ptr);
+    a.results = static_cast<ce_result*>(t->d_results.ptr);
+    a.counter = bk.counters;
+    a.order = bk.order;
+    a.bounds = bk.bounds;
+    a.work = bk.work;
+    a.queues = cek::kQueues;
+    a.count = (uint32_t)t->count;
+    a.rows = t->rows;
+    a.mm = t->mm;
+    a.chunk_k = t->engine->chunk_k;
+    a.ckpt = static_cast<float*>(t->d_ckpt.ptr);
+    a.ckpt_stride = t->ckpts * cek::checkpoint_floats(t->rows, t->mm);
+    a.ends = static_cast<uint32_t*>(t->d_ends.ptr);
+    return a;
+}
+
+}  // namespace
+
+extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce_world* w, uint32_t checkpoint_every,
+                                ce_tape** out) {
+    if (!e || !pack || !out || !pack->count) {
+        set_error("ce_forward: null argument or empty batch");
+        return CE_ERR_INVALID;
+    }
+    *out = nullptr;
+    ce_status s = check_world(w);
+    if (s != CE_OK) return s;
+    if (ce_world_flags(w) != cek::kWorldCalm) {
+        set_error("ce_forward: gradients are built for the calm world (flat ground, no effects)");
+        return CE_ERR_UNSUPPORTED;
+    }
+    if (checkpoint_every != 256u) {
+        set_error("ce_forward: checkpoints come every 256 substeps");
+        return CE_ERR_UNSUPPORTED;
+    }
+    std::vector<ClassPlan> plans;
+    if ((s = plan_classes(pack, plans)) != CE_OK) return s;
+    for (size_t k = 0; k < pack->muscles_len / CE_MUSCLE_FIELDS; k++) {
+        uint32_t sensor;
+        std::memcpy(&sensor, pack->muscles + k * CE_MUSCLE_FIELDS + 16, 4);
+        if (sensor != CE_NONE) {
+            set_error("ce_forward: muscles with touch sensors are not differentiated");
+            return CE_ERR_UNSUPPORTED;
+        }
+    }
+    ce_tape* t = new ce_tape;
+    t->engine = e;
+    t->count = pack->count;
+    for (const ClassPlan& c : plans) {
+        t->rows = std::max(t->rows, c.rows);
+        t->mm = std::max(t->mm, c.mm);
+    }
+    t->rate = (int)ce::world_rate(*w);
+    ce_make_params(w, 0, (uint32_t)pack->count, 0, &t->params);
+    t->ckpts = (t->params.steps + 15u) / 16u;
+    auto fail = [&](ce_status st) {
+        ce_tape_free(t);
+        return st;
+    };
+    if ((s = set_device(e)) != CE_OK) return fail(s);
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (s = cuda_status(cudaEventCreate(&t->start), "cudaEventCreate")) ||
+        (s = cuda_status(cudaEventCreate(&t->stop), "cudaEventCreate"))) {
+        return fail(s);
+    }
+    const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
+    const size_t res_b = pack->count * sizeof(ce_result);
+    const size_t ckpt_b = pack->count * (size_t)t->ckpts * cek::checkpoint_floats(t->rows, t->mm) * 4;
+    t->grid = grid_for(e, t->rows, t->mm, cek::kWorldCalm, false, t->rate, pack->count);
+    if ((s = t->d_lanes.ensure(lanes_b)) || (s = t->d_muscles.ensure(std::max<size_t>(mus_b, 4))) ||
+        (s = t->d_heads.ensure(heads_b)) || (s = t->d_results.ensure(res_b)) ||
+        (s = t->d_buckets.ensure(cek::bucket_bytes(pack->count))) || (s = t->d_ckpt.ensure(ckpt_b)) ||
+        (s = t->d_ends.ensure(pack->count * 4)) ||
+        (s = t->d_scratch.ensure(scratch_bytes(t->grid, t->rows, t->mm, false)))) {
+        return fail(s);
+    }
+    cudaStream_t st = t->stream;
+    if ((s = cuda_status(cudaMemcpyAsync(t->d_lanes.ptr, pack->lanes, lanes_b, cudaMemcpyHostToDevice, st),
+                         "cudaMemcpyAsync")) ||
+        (s = cuda_status(cudaMemcpyAsync(t->d_muscles.ptr, pack->muscles, mus_b, cudaMemcpyHostToDevice, st),
+                         "cudaMemcpyAsync")) ||
+        (s = cuda_status(cudaMemcpyAsync(t->d_heads.ptr, pack->heads, heads_b, cudaMemcpyHostToDevice, st),
+                         "cudaMemcpyAsync")) ||
+        (s = cuda_status(cudaMemsetAsync(t->d_ends.ptr, 0, pack->count * 4, st), "cudaMemsetAsync"))) {
+        return fail(s);
+    }
+    const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, pack->count);
+    if ((s = cuda_status(cudaEventRecord(t->start, st), "cudaEventRecord")) ||
+        (s = cuda_status(cek::launch_bucket(static_cast<const uint4*>(t->d_heads.ptr), 0u, (uint32_t)pack->count,
+                                            bk, st),
+                         "bucketing launch"))) {
+        return fail(s);
+    }
+    cek::KernelArgs a = tape_args(t, bk);
+    a.scratch = static_cast<float4*>(t->d_scratch.ptr);
+    cek::LaunchSpec ls{t->rows, t->mm, cek::kWorldCalm, false, t->rate, t->grid, cek::kBlock, st};
+    if ((s = cuda_status(cek::launch_forward_ckpt(ls, a, t->params), "forward launch")) ||
+        (s = cuda_status(cudaEventRecord(t->stop, st), "cudaEventRecord")) ||
+        (s = tape_time(t, &t->forward_seconds))) {
+        return fail(s);
+    }
+    t->results.resize(pack->count);
+    if ((s = cuda_status(cudaMemcpy(t->results.data(), t->d_results.ptr, res_b, cudaMemcpyDeviceToHost),
+                         "cudaMemcpy"))) {
+        return fail(s);
+    }
+    *out = t;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_tape_results(ce_tape* t, ce_result* out, size_t cap) {
+    if (!t || !out || cap < t->count) {
+        set_error("ce_tape_results: null argument or buffer too small");
+        return CE_ERR_INVALID;
+    }
+    std::memcpy(out, t->results.data(), t->count * sizeof(ce_result));
+    return CE_OK;
+}
+
+extern "C" uint32_t ce_tape_grad_floats(ce_tape* t) { return t ? cek::grad_floats(t->rows, t->mm) : 0u; }
+
+extern "C" ce_status ce_tape_seconds(ce_tape* t, double* forward, double* backward) {
+    if (!t) return CE_ERR_INVALID;
+    if (forward) *forward = t->forward_seconds;
+    if (backward) *backward = t->backward_seconds;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* grads, size_t cap_floats) {
+    if (!t || !grads) {
+        set_error("ce_backward: null argument");
+        return CE_ERR_INVALID;
+    }
+    const size_t per = cek::grad_floats(t->rows, t->mm);
+    if (cap_floats < t->count * per) {
+        set_error("ce_backward: gradient buffer too small, need " + std::to_string(t->count * per) + " floats");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = set_device(t->engine);
+    if (s != CE_OK) return s;
+    int per_sm = 0;
+    if (cek::adjoint_occupancy(t->rows, t->mm, t->rate, &per_sm) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const size_t needed = (t->count + cek::kBlock - 1) / cek::kBlock;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min(needed, (size_t)per_sm * t->engine->sms));
+    const size_t slot_b = cek::adjoint_slot_bytes(grid, t->rows, t->mm);
+    const size_t grads_b = t->count * per * 4;
+    if ((s = t->d_scratch.ensure(slot_b)) || (s = t->d_tape.ensure(cek::adjoint_tape_bytes(grid, t->rows, t->mm))) ||
+        (s = t->d_grads.ensure(grads_b)) || (s = t->d_weights.ensure(t->count * 4))) {
+        return s;
+    }
+    cudaStream_t st = t->stream;
+    if (dl_dfitness) {
+        CE_TRY(cudaMemcpyAsync(t->d_weights.ptr, dl_dfitness, t->count * 4, cudaMemcpyHostToDevice, st),
+               "cudaMemcpyAsync");
+    }
+    CE_TRY(cudaMemsetAsync(t->d_grads.ptr, 0, grads_b, st), "cudaMemsetAsync");
+    CE_TRY(cudaEventRecord(t->start, st), "cudaEventRecord");
+    const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, t->count);
+    CE_TRY(cek::launch_bucket(static_cast<const uint4*>(t->d_heads.ptr), 0u, (uint32_t)t->count, bk, st),
+           "bucketing launch");
+    cek::KernelArgs a = tape_args(t, bk);
+    a.scratch = static_cast<float4*>(t->d_scratch.ptr);
+    cek::LaunchSpec ls{t->rows, t->mm, cek::kWorldCalm, false, t->rate, grid, cek::kBlock, st};
+    CE_TRY(cek::launch_adjoint(ls, a, t->params, static_cast<float4*>(t->d_tape.ptr),
+                               static_cast<float*>(t->d_grads.ptr),
+                               dl_dfitness ? static_cast<const float*>(t->d_weights.ptr) : nullptr),
+           "backward launch");
+    CE_TRY(cudaEventRecord(t->stop, st), "cudaEventRecord");
+    if ((s = tape_time(t, &t->backward_seconds)) != CE_OK) return s;
+    CE_TRY(cudaMemcpy(grads, t->d_grads.ptr, grads_b, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CE_OK;
+}
+
+extern "C" ce_status ce_tape_free(ce_tape* t) {
+    if (!t) return CE_OK;
+    if (t->engine) cudaSetDevice(t->engine->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    for (DeviceBuf* b : {&t->d_lanes, &t->d_muscles, &t->d_heads, &t->d_results, &t->d_buckets, &t->d_ckpt,
+                         &t->d_ends, &t->d_scratch, &t->d_tape, &t->d_grads, &t->d_weights}) {
+        b->release();
+    }
+    if (t->start) cudaEventDestroy(t->start);
+    if (t->stop) cudaEventDestroy(t->stop);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_tape_shape(ce_tape* t, uint32_t* rows, uint32_t* muscle_slots) {
+    if (!t) return CE_ERR_INVALID;
+    if (rows) *rows = t->rows;
+    if (muscle_slots) *muscle_slots = t->mm;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_tape_checkpoints(ce_tape* t, float* out, size_t cap_floats, uint32_t* per_creature) {
+    if (!t || !out) return CE_ERR_INVALID;
+    const size_t per = (size_t)t->ckpts * cek::checkpoint_floats(t->rows, t->mm);
+    if (cap_floats < per * t->count) {
+        set_error("ce_tape_checkpoints: buffer too small, need " + std::to_string(per * t->count) + " floats");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = set_device(t->engine);
+    if (s != CE_OK) return s;
+    CE_TRY(cudaMemcpy(out, t->d_ckpt.ptr, per * t->count * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (per_creature) *per_creature = t->ckpts;
+    return CE_OK;
+}

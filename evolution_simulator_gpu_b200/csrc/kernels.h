@@ -57,7 +57,34 @@ struct KernelArgs {
     uint32_t mm;                   // most muscles of a body of this launch
     uint32_t frames_per_creature;  // RECORD: frames of one recording
     uint32_t chunk_k;              // claims shrink to 1 / chunk_k of the rest per warp
+    float* ckpt;                   // CKPT: checkpoints, ckpt_stride floats a creature (packed index)
+    uint32_t ckpt_stride;
+    uint32_t* ends;                // CKPT: steps each creature's trial ran (packed index)
 };
+
+// Floats of one checkpoint: positions and velocities of `rows` nodes, then
+// the energy stores of `mm` muscles.
+__host__ __device__ inline unsigned checkpoint_floats(unsigned rows, unsigned mm) { return 4u * rows + mm; }
+
+// Gradient of one creature's fitness per record field: for each of `mm`
+// muscles the stroke amplitude, hill factor, force cap, inverse energy
+// capacity, phase, duty, 1 / duty, 1 / (1 - duty) and stiffness, then the
+// friction of each of `rows` nodes, then each node's mass (through every
+// place the kernel uses a mass or an inverse mass and the fitness's mass
+// weighting), then each node's start position (x, y).
+constexpr unsigned kGradMuscle = 9u;
+__host__ __device__ inline unsigned grad_floats(unsigned rows, unsigned mm) { return kGradMuscle * mm + 4u * rows; }
+
+// Gradient kernels (calm world): the creature kernel with checkpoints every
+// 256 substeps (KernelArgs::ckpt, ends), and the backward kernel.
+size_t adjoint_smem_bytes(unsigned rows, unsigned mm, unsigned block);
+size_t adjoint_slot_bytes(unsigned grid, unsigned rows, unsigned mm);   // lane slots of the backward grid
+size_t adjoint_tape_bytes(unsigned grid, unsigned rows, unsigned mm);   // segment tapes of the backward grid
+cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, int rate, int* blocks);
+struct LaunchSpec;
+cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
+cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
+                           const float* weights);
 
 // The device arrays that bucketing writes for `count` creatures, carved from
 // one area of bucket_bytes(count) bytes.

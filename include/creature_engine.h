@@ -304,6 +304,49 @@ ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const fl
                             uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
                             void* stream);
 
+/* Gradients of fitness (no counterpart in the reference, which has no
+ * derivatives): a forward/backward pair shaped like an autograd function.
+ * ce_forward runs the batch in the calm world (flat ground, no effects;
+ * CE_ERR_UNSUPPORTED otherwise, or for muscles with touch sensors) with a
+ * checkpoint of each creature's state every `checkpoint_every` substeps
+ * (256 only) and keeps what the backward pass needs in the tape; its results
+ * equal ce_submit's to the bit. ce_backward returns, for every creature in
+ * packed order, d(sum_c dl_dfitness[c] * fitness_c) with respect to the
+ * creature's record fields: ce_tape_grad_floats(tape) floats a creature,
+ * first 9 a muscle slot (stroke amplitude, hill factor, force cap,
+ * 1 / energy capacity, phase, duty, 1 / duty, 1 / (1 - duty), stiffness;
+ * muscle slots up to the batch's largest muscle count), then per node row
+ * (rows up to the largest node count) its friction, then its mass, then its
+ * start position as (x, y) pairs. `dl_dfitness` NULL means 1
+ * for every creature. Both are synchronous; ce_tape_seconds gives their
+ * GPU time. ce_gene_gradients maps the record gradients to genes. */
+typedef struct ce_tape ce_tape;
+ce_status ce_forward(ce_engine* engine, const ce_wave_pack* pack, const ce_world* world,
+                     uint32_t checkpoint_every, ce_tape** tape);
+ce_status ce_tape_results(ce_tape* tape, ce_result* out, size_t cap);
+uint32_t ce_tape_grad_floats(ce_tape* tape);
+ce_status ce_tape_seconds(ce_tape* tape, double* forward_seconds, double* backward_seconds);
+ce_status ce_backward(ce_tape* tape, const float* dl_dfitness, float* grads, size_t cap_floats);
+ce_status ce_tape_free(ce_tape* tape);
+/* The forward run's checkpoints, for checking: per creature (packed order)
+ * ceil(steps / 16) checkpoints of rows x 4 + muscle slots floats (positions
+ * and velocities of each node row as (x, y) pairs, then the muscles' energy
+ * stores), `per_creature` receiving the checkpoint count. */
+ce_status ce_tape_checkpoints(ce_tape* tape, float* out, size_t cap_floats, uint32_t* per_creature);
+/* Node rows and muscle slots of the tape's gradient records. */
+ce_status ce_tape_shape(ce_tape* tape, uint32_t* rows, uint32_t* muscle_slots);
+/* Gene gradients of the creatures of a batch packed by ce_pack(pop,
+ * indices, n, world, ..., slots, ...), from its record gradients `grads`
+ * (rows and muscle slots as ce_tape_shape gives): for each muscle gene 5
+ * doubles at muscle_grads[5 * muscle index] (d/d short length, long length,
+ * strength scale, on time, off time, the period held fixed; on time and off
+ * time give phase = frac(-on / period) and duty = frac((off - on) / period)
+ * clamped to [0.05, 0.95]), and d/d friction at node_grads[node index]. */
+ce_status ce_gene_gradients(const ce_population* pop, const uint32_t* indices, size_t n,
+                            const ce_world* world, const uint32_t* slots, const float* grads,
+                            uint32_t rows, uint32_t muscle_slots, double* muscle_grads,
+                            double* node_grads);
+
 /* The device-level entry above for a caller that cannot allocate GPU memory:
  * no counterpart in the reference. It allocates nothing: the kernel's
  * scratch (claim counter and lane slots) is a fixed array of

@@ -89,6 +89,24 @@ struct Sim {
         bool at_head;
         T lo, hi, mid, wt, wf, wh;
     };
+    T fit_t = T(0.0f);  // the fitness as a T (its derivative parts for a dual T)
+    const double* seed_mass = nullptr;  // dual T: node-mass directions set in begin
+    // Checkpoints of another run of the same trial (positions, velocities,
+    // energy stores every `resync_every` substeps, rows x 4 + mm floats
+    // each): when set, the state's values are reset to them at each
+    // checkpoint, its derivative parts kept, so the run follows that
+    // trajectory.
+    const float* resync = nullptr;
+    uint32_t resync_rows = 0, resync_mm = 0, resync_count = 0, resync_every = 256;
+    void resync_state(const float* c) {
+        for (uint32_t i = 0; i < N; i++) {
+            set_value(px[i], c[2 * i]);
+            set_value(py[i], c[2 * i + 1]);
+            set_value(vx[i], c[2 * resync_rows + 2 * i]);
+            set_value(vy[i], c[2 * resync_rows + 2 * i + 1]);
+        }
+        for (uint32_t k = 0; k < M; k++) set_value(mus[k].energy, c[4 * resync_rows + k]);
+    }
     struct Muscle {
         uint32_t a0, a1, b0, b1, sensor;
         T aa, ab, hill, cap, icap, tk, slack, amp, iper, phase, duty, iduty, icomp, stiff, reset;
@@ -210,11 +228,18 @@ struct Sim {
         feet = 0;
         for (uint32_t i = 0; i < N; i++) {
             const uint32_t* r = rec + i * 6;
-            const T m = T(fbits(r[0]));
+            T m = T(fbits(r[0]));
+            if (seed_mass) set_deriv(m, seed_mass[i]);
             node[i] = Node{m, T(1.0f) / m, T(fbits(r[1])), T(fbits(r[2]))};
             px[i] = T(fbits(r[3]));
             py[i] = T(fbits(r[4]));
             feet |= (r[5] & 1u) << i;
+        }
+        if (seed_mass) {
+            // inv_mass = 1 / sum of node masses.
+            double dsum = 0.0;
+            for (uint32_t i = 0; i < N; i++) dsum += seed_mass[i];
+            set_deriv(inv_mass, -dsum * (double)fbits(h1[2]) * (double)fbits(h1[2]));
         }
         const uint32_t* bone_rec = rec + N * 6;
         const uint32_t B = N - 1;
@@ -547,7 +572,13 @@ struct Sim {
         for (uint32_t step = 0;; step++) {
             const T t_now = T((float)step) * dt;
             muscle_demands(t_now, false);
-            for (int s = 0; s < 16; s++) substep();
+            for (uint32_t s = 0; s < 16u; s++) {
+                const uint32_t k = step * 16u + s;
+                if (resync && k % resync_every == 0u && k / resync_every < resync_count) {
+                    resync_state(resync + (size_t)(k / resync_every) * (4u * resync_rows + resync_mm));
+                }
+                substep();
+            }
             if (trace && step < trace_steps) {
                 for (uint32_t i = 0; i < N; i++) {
                     trace[(step * 32 + i) * 2] = to_f(px[i]);
@@ -607,6 +638,7 @@ struct Sim {
             if (fell) {
                 mt.fall_time = to_f(t_now + dt);
                 mt.fitness = failed ? -1e20f : to_f(com_x);
+                fit_t = failed ? T(0.0f) : com_x;
                 if (step <= p.screen_step) mt.screen_x = mt.fitness;
                 ended = true;
             }
@@ -682,6 +714,7 @@ struct Sim {
                         mt.screened = to_f(t_now + dt);
                         mt.screen_x = comf;
                         mt.fitness = comf;
+                        fit_t = com_x;
                         rung_bits |= (rr + 1) << 6;
                         ended = true;
                     }
@@ -700,6 +733,7 @@ struct Sim {
                 if (comf < bar && (cflags & 1u) == 0u) {
                     mt.screened = to_f(t_now + dt);
                     mt.fitness = comf;
+                    fit_t = com_x;
                     ended = true;
                 }
             }
@@ -709,6 +743,7 @@ struct Sim {
                 gf = turns * T(0.5f) / (t_now + dt);
             } else if (step + 1 >= p.steps) {
                 mt.fitness = comf;
+                fit_t = com_x;
                 vo = max_(gf - vo, T(0.0f));
                 gf = turns * T(0.5f) / max_(T((float)(step + 1)) * dt, dt);
                 last = true;
@@ -748,6 +783,39 @@ void simulate(const uint32_t* records, const float* muscles, const uint32_t* hea
     Sim<T> s(p, flags, rate);
     s.begin(records, muscles, heads, cidx);
     s.run(*out, trace, trace_steps);
+}
+
+double tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t cidx, const Params& p,
+               uint32_t flags, int rate, const double* dmuscle, const double* dnode, Result* out,
+               const float* resync, uint32_t rows, uint32_t mm, uint32_t count, uint32_t every, double* fitness,
+               const double* dmass) {
+    Sim<Dual> s(p, flags, rate);
+    s.seed_mass = dmass;
+    s.begin(records, muscles, heads, cidx);
+    s.resync_every = every > 0 ? every : 256u;
+    s.resync = resync;
+    s.resync_rows = rows;
+    s.resync_mm = mm;
+    s.resync_count = count;
+    for (size_t k = 0; k < s.mus.size(); k++) {
+        auto& u = s.mus[k];
+        const double* d = dmuscle + 9 * k;
+        u.amp.d = d[0];
+        u.hill.d = d[1];
+        u.cap.d = d[2];
+        u.icap.d = d[3];
+        u.phase.d = d[4];
+        u.duty.d = d[5];
+        u.iduty.d = d[6];
+        u.icomp.d = d[7];
+        u.stiff.d = d[8];
+    }
+    for (size_t i = 0; i < s.node.size(); i++) {
+        s.node[i].mu.d = dnode[i];
+    }
+    s.run(*out, nullptr, 0);
+    if (fitness) *fitness = s.fit_t.v;
+    return s.fit_t.d;
 }
 
 template void simulate<float>(const uint32_t*, const float*, const uint32_t*, size_t, const Params&, uint32_t, int,
@@ -790,6 +858,46 @@ void oracle_trace(const uint32_t* records, const float* muscles, const uint32_t*
     } else {
         oracle::simulate<float>(records, muscles, heads, cidx, *p, flags, rate, out, trace, trace_steps);
     }
+}
+
+// FP64 tangents of creatures [first, first + n): for creature c the record
+// directions sit at dmuscle + c * 9 * mm and dnode + c * rows; d fitness goes
+// to dfit[c] and the FP64 fitness to fit[c] (when not NULL). `dmass` (NULL
+// for none, else rows a creature) moves the node masses too. Returns the wall
+// seconds.
+double oracle_tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t first, size_t n,
+                      const oracle::Params* p, uint32_t flags, int rate, const double* dmuscle, const double* dnode,
+                      uint32_t rows, uint32_t mm, double* dfit, double* fit, oracle::Result* out, int threads,
+                      const double* dmass) {
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long i = 0; i < (long long)n; i++) {
+        dfit[i] = oracle::tangent(records, muscles, heads, first + i, *p, flags, rate, dmuscle + i * 9 * mm,
+                                  dnode + i * rows, out + i, nullptr, 0, 0, 0, 256, fit ? fit + i : nullptr,
+                                  dmass ? dmass + i * rows : nullptr);
+    }
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// As oracle_tangent, the state reset at every checkpoint to `ckpt` (per
+// creature `count` checkpoints of rows x 4 + mm floats, one every `every`
+// substeps, creature c's at ckpt + c * ckpt_stride): the FP64 tangent along
+// another run's trajectory.
+double oracle_tangent_along(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t first,
+                            size_t n, const oracle::Params* p, uint32_t flags, int rate, const double* dmuscle,
+                            const double* dnode, uint32_t rows, uint32_t mm, const float* ckpt, size_t ckpt_stride,
+                            uint32_t count, uint32_t every, double* dfit, double* fit, oracle::Result* out,
+                            int threads, const double* dmass) {
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long i = 0; i < (long long)n; i++) {
+        dfit[i] = oracle::tangent(records, muscles, heads, first + i, *p, flags, rate, dmuscle + i * 9 * mm,
+                                  dnode + i * rows, out + i, ckpt + (first + i) * ckpt_stride, rows, mm, count,
+                                  every, fit ? fit + i : nullptr, dmass ? dmass + i * rows : nullptr);
+    }
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Counts the arithmetic of creature `cidx`'s trial: out[0..7] = add, mul,

@@ -74,6 +74,45 @@ inline Counted max_(Counted a, Counted b) { g_ops.minmax++; return Counted(std::
 inline float copysign_(float a, float b) { return std::copysign(a, b); }
 inline double copysign_(double a, double b) { return std::copysign(a, b); }
 inline Counted copysign_(Counted a, Counted b) { g_ops.other++; return Counted(std::copysign(a.v, b.v)); }
+// FP64 dual number: value and one directional derivative (forward mode).
+struct Dual {
+    double v = 0.0, d = 0.0;
+    Dual() = default;
+    Dual(double x) : v(x), d(0.0) {}
+    Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(Dual a, Dual b) { return Dual(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
+inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
+inline Dual& operator*=(Dual& a, Dual b) { a = a * b; return a; }
+inline Dual& operator/=(Dual& a, Dual b) { a = a / b; return a; }
+inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
+inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
+inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
+inline bool operator==(Dual a, Dual b) { return a.v == b.v; }
+inline bool operator!=(Dual a, Dual b) { return a.v != b.v; }
+inline Dual sqrt_(Dual x) {
+    const double s = std::sqrt(x.v);
+    return Dual(s, s > 0.0 ? x.d / (2.0 * s) : 0.0);
+}
+inline Dual cos_(Dual x) { return Dual(std::cos(x.v), -std::sin(x.v) * x.d); }
+inline Dual atan2_(Dual y, Dual x) {
+    const double r = x.v * x.v + y.v * y.v;
+    return Dual(std::atan2(y.v, x.v), r > 0.0 ? (x.v * y.d - y.v * x.d) / r : 0.0);
+}
+inline Dual floor_(Dual x) { return Dual(std::floor(x.v), 0.0); }
+inline Dual abs_(Dual x) { return x.v < 0.0 ? -x : x; }
+inline Dual min_(Dual a, Dual b) { return b.v < a.v ? b : a; }
+inline Dual max_(Dual a, Dual b) { return b.v > a.v ? b : a; }
+inline Dual copysign_(Dual a, Dual b) { return std::signbit(a.v) == std::signbit(b.v) ? a : -a; }
+inline float to_f(Dual x) { return (float)x.v; }
+inline bool finite_(Dual x) { return std::isfinite(x.v); }
+
 inline float to_f(float x) { return x; }
 inline float to_f(double x) { return (float)x; }
 inline float to_f(Counted x) { return x.v; }
@@ -111,5 +150,32 @@ enum : uint32_t {
 template <class T>
 void simulate(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t cidx, const Params& p,
               uint32_t flags, int rate, Result* out, float* trace, size_t trace_steps);
+
+// FP64 tangent of creature `cidx`'s fitness: the trial run in dual numbers
+// with the record fields moved along `dmuscle` (9 a muscle: amplitude, hill,
+// cap, 1/capacity, phase, duty, 1/duty, 1/(1-duty), stiffness) and `dnode`
+// (friction a node row) and, when not NULL, the node masses along `dmass`
+// (a node row each; 1/m, the bone and joint weights and 1/total mass follow).
+// Returns d fitness; `out` gets the FP64 trial's result and `fitness` (when
+// not NULL) its fitness in FP64.
+// With `resync` (count checkpoints of rows x 4 + mm floats: positions,
+// velocities, energy stores every `every` substeps) the state's values are
+// reset to them at each checkpoint and their derivative parts kept.
+double tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t cidx, const Params& p,
+               uint32_t flags, int rate, const double* dmuscle, const double* dnode, Result* out,
+               const float* resync, uint32_t rows, uint32_t mm, uint32_t count, uint32_t every,
+               double* fitness, const double* dmass);
+
+// The value part of a scalar of the oracle (for dual numbers: keeps the
+// derivative).
+inline void set_value(float& x, float v) { x = v; }
+inline void set_value(double& x, float v) { x = v; }
+inline void set_value(Counted& x, float v) { x = Counted(v); }
+inline void set_value(Dual& x, float v) { x.v = v; }
+// The derivative part of a scalar (dual numbers only).
+inline void set_deriv(float&, double) {}
+inline void set_deriv(double&, double) {}
+inline void set_deriv(Counted&, double) {}
+inline void set_deriv(Dual& x, double d) { x.d = d; }
 
 }  // namespace oracle

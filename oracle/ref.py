@@ -87,6 +87,16 @@ class Oracle:
         self.lib.oracle_trace.restype = None
         self.lib.oracle_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32,
                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]
+        self.lib.oracle_tangent.restype = C.c_double
+        self.lib.oracle_tangent.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p,
+                                            C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        self.lib.oracle_tangent_along.restype = C.c_double
+        self.lib.oracle_tangent_along.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t,
+                                                  C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p,
+                                                  C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t, C.c_uint32,
+                                                  C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                  C.c_void_p]
         self.lib.oracle_count.restype = None
         self.lib.oracle_count.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32,
                                           C.c_int, C.c_void_p, C.c_void_p]
@@ -116,3 +126,48 @@ class Oracle:
         self.lib.oracle_count(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data, cidx,
                               C.byref(params), flags, rate, out.ctypes.data, counts.ctypes.data)
         return out[0], counts
+
+    def tangent(self, wave, params, flags: int, dmuscle, dnode, rate: int = 60, first: int = 0, threads: int = 0,
+                dmass=None):
+        """FP64 forward-mode tangents of the fitness of packed creatures
+        [first, first + n): creature c's record fields move along
+        dmuscle[c] (muscle slots x 9: amplitude, hill, cap, 1/capacity, phase,
+        duty, 1/duty, 1/(1-duty), stiffness) and dnode[c] (node rows:
+        friction) and dmass[c] (node rows: mass; None for none). Returns
+        (d fitness [n], FP64 results, wall seconds); the FP64 fitness itself
+        is left in `self.fitness64`."""
+        dm = np.ascontiguousarray(dmuscle, np.float64)
+        dn = np.ascontiguousarray(dnode, np.float64)
+        n, mm = dm.shape[0], dm.shape[1]
+        rows = dn.shape[1]
+        out = np.zeros(n, RESULT_DTYPE)
+        dfit = np.zeros(n, np.float64)
+        fit = np.zeros(n, np.float64)
+        secs = self.lib.oracle_tangent(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data,
+                                       first, n, C.byref(params), flags, rate, dm.ctypes.data, dn.ctypes.data, rows,
+                                       mm, dfit.ctypes.data, fit.ctypes.data, out.ctypes.data, threads,
+                                       None if dmass is None else np.ascontiguousarray(dmass, np.float64).ctypes.data)
+        self.fitness64 = fit
+        return dfit, out, secs
+
+    def tangent_along(self, wave, params, flags: int, dmuscle, dnode, checkpoints, rate: int = 60,
+                      threads: int = 0, every: int = 256, dmass=None):
+        """As tangent, for packed creatures [0, n), with the FP64 state's
+        values reset every `every` substeps to another run's `checkpoints`
+        [creature, checkpoint, rows x 4 + muscle slots] (a GPU forward run's):
+        the FP64 tangent along that run's trajectory."""
+        dm = np.ascontiguousarray(dmuscle, np.float64)
+        dn = np.ascontiguousarray(dnode, np.float64)
+        ck = np.ascontiguousarray(checkpoints, np.float32)
+        n, mm = dm.shape[0], dm.shape[1]
+        rows = dn.shape[1]
+        assert ck.shape[0] >= n and ck.shape[2] == 4 * rows + mm
+        out = np.zeros(n, RESULT_DTYPE)
+        dfit = np.zeros(n, np.float64)
+        secs = self.lib.oracle_tangent_along(wave.lanes.ctypes.data, wave.muscles.ctypes.data,
+                                             wave.heads.ctypes.data, 0, n, C.byref(params), flags, rate,
+                                             dm.ctypes.data, dn.ctypes.data, rows, mm, ck.ctypes.data,
+                                             ck.shape[1] * ck.shape[2], ck.shape[1], every, dfit.ctypes.data, None,
+                                             out.ctypes.data, threads,
+                                             None if dmass is None else np.ascontiguousarray(dmass, np.float64).ctypes.data)
+        return dfit, out, secs

@@ -1,0 +1,159 @@
+"""The gradient path on the GPU (ce_forward / ce_backward) against the FP64
+dual-number tangent of the host physics and FP64 finite differences.
+
+The backward kernel differentiates the FP32 trajectory the forward kernel
+took, through its contact, stick/slip, joint-limit and clamp modes. The FP64
+tangent (oracle/creature_oracle.cpp) differentiates the FP64 trajectory of
+the same trial; the two agree while the trajectories take the same modes,
+which holds for nearly every creature over a few steps and for fewer as the
+trial grows (a mode taken differently near a threshold changes the
+derivative), so the checks below are on short trials. Central differences
+of the FP32 kernel are not a usable check: its trajectories respond to
+record changes below about 1e-2 relative with rounding noise.
+"""
+import numpy as np
+import pytest
+
+import evolution_simulator_gpu_b200 as ce
+from evolution_simulator_gpu_b200.configs import WORKLOADS, effects_world_kw
+from oracle.ref import Oracle
+
+pytestmark = pytest.mark.gpu
+
+W = WORKLOADS["gradients"]
+
+
+def _record_direction(wave, rows, mm, rng):
+    dm = rng.normal(size=(len(wave), mm, 9))
+    dn = rng.normal(size=(len(wave), rows))
+    dmass = rng.normal(size=(len(wave), rows)) * 0.01
+    for c in range(len(wave)):
+        dm[c, int(wave.heads[c, 1]):] = 0.0
+        dn[c, int(wave.heads[c, 0] & 255):] = 0.0
+        dmass[c, int(wave.heads[c, 0] & 255):] = 0.0
+    return dm, dn, dmass
+
+
+def _project(g, rows, mm, dm, dn, dmass):
+    g = g.astype(np.float64)
+    n = len(g)
+    return ((g[:, :9 * mm].reshape(n, mm, 9) * dm).sum(axis=(1, 2)) + (g[:, 9 * mm:9 * mm + rows] * dn).sum(axis=1)
+            + (g[:, 9 * mm + rows:9 * mm + 2 * rows] * dmass).sum(axis=1))
+
+
+def test_forward_results_equal_the_plain_kernel(engine):
+    world = W.world(duration=2.0)
+    wave = ce.pack(ce.generate(W.spec, 4096), world)
+    plain, _ = engine.run(wave, world)
+    with engine.forward(wave, world) as tape:
+        res = tape.results
+    assert (res.view(np.uint32) == plain.view(np.uint32)).all()
+
+
+@pytest.mark.parametrize("seconds,median,share", [(0.05, 1e-4, 0.95), (0.25, 1e-3, 0.55)])
+def test_adjoint_matches_fp64_tangent(engine, seconds, median, share):
+    """<gradient, u> against the FP64 tangent along u for 256 creatures, u a
+    random direction in all record fields (muscles, friction, mass)."""
+    world = W.world(duration=seconds)
+    wave = ce.pack(ce.generate(W.spec, 256), world)
+    with engine.forward(wave, world) as tape:
+        g = tape.backward()
+        rows, mm = tape.shape
+        res = tape.results
+    dm, dn, dmass = _record_direction(wave, rows, mm, np.random.default_rng(7))
+    tangent, _, _ = Oracle().tangent(wave, ce.make_params(world), ce.world_flags(world), dm, dn, dmass=dmass)
+    adj = _project(g, rows, mm, dm, dn, dmass)
+    ok = res["fitness"] > -1e19
+    rel = np.abs(adj - tangent)[ok] / np.maximum(np.abs(tangent[ok]), 1e-12)
+    assert np.median(rel) < median, np.median(rel)
+    assert (rel < 1e-3).mean() >= share, (rel < 1e-3).mean()
+
+
+def test_gene_gradients_match_fp64_differences(engine):
+    """End to end: GPU record gradient, gene chain rule, against central
+    differences of the FP64 host physics over repacked genes (h = 2e-4,
+    mode-preserving perturbations: the one-sided differences agree)."""
+    world = W.world(duration=0.1)
+    pop = ce.generate(W.spec, 64)
+    wave = ce.pack(pop, world)
+    with engine.forward(wave, world) as tape:
+        g = tape.backward()
+        shape = tape.shape
+    mg, ng = ce.gene_gradients(pop, wave, world, g, shape)
+    rng = np.random.default_rng(11)
+    o = Oracle()
+    p, flags = ce.make_params(world), ce.world_flags(world)
+    checked = agree = 0
+    for c in range(len(wave)):
+        i = int(wave.slots[c])
+        one = pop.subset([i])
+        m = one.muscles
+        vm = rng.normal(size=(len(m), 5))
+        vn = rng.normal(size=len(one.nodes))
+        # No on/off move where duty sits at its clamp or phase near its wrap.
+        kink = (m["duty"] <= 0.0501) | (m["duty"] >= 0.9499) | (m["phase"] < 0.01) | (m["phase"] > 0.99)
+        vm[kink, 3:] = 0.0
+
+        def fitness(h):
+            mm_ = m.copy()
+            nn = one.nodes.copy()
+            T = mm_["period"].astype(np.float64)
+            mm_["short"] = (mm_["short"] + h * vm[:, 0]).astype(np.float32)
+            mm_["long"] = (mm_["long"] + h * vm[:, 1]).astype(np.float32)
+            mm_["phase"] = (mm_["phase"] - h * vm[:, 3] / T).astype(np.float32)
+            mm_["duty"] = (mm_["duty"] + h * (vm[:, 4] - vm[:, 3]) / T).astype(np.float32)
+            nn["friction"] = (nn["friction"] + h * vn).astype(np.float32)
+            st = (one.strength + h * vm[:, 2]).astype(np.float32)
+            w1 = ce.pack(ce.Population(nn, one.bones, mm_, one.genomes, st), world)
+            o.tangent(w1, p, flags, np.zeros((1, int(w1.heads[0, 1]), 9)), np.zeros((1, int(w1.heads[0, 0] & 255))))
+            return float(o.fitness64[0])
+
+        h = 2e-4
+        f0, fp, fm = fitness(0.0), fitness(h), fitness(-h)
+        up, down = (fp - f0) / h, (f0 - fm) / h
+        if abs(up - down) > 0.05 * max(abs(up), abs(down)) + 1e-9:
+            continue
+        fd = (fp - fm) / (2 * h)
+        gs = pop.genomes[i]
+        got = float((mg[gs["muscle_start"]:gs["muscle_start"] + gs["muscle_count"]] * vm).sum()
+                    + (ng[gs["node_start"]:gs["node_start"] + gs["node_count"]] * vn).sum())
+        checked += 1
+        agree += abs(got - fd) <= 2e-2 * max(abs(fd), 1e-6)
+    assert checked >= 24, checked
+    assert agree >= 0.8 * checked, (agree, checked)
+
+
+def test_backward_is_linear_in_the_fitness_weights(engine):
+    """Weights scale each creature's gradient (up to FP32 rounding, compared
+    where the gradient is moderate: trials whose gradients explode through
+    near-degenerate joint configurations amplify rounding)."""
+    world = W.world(duration=0.25)
+    wave = ce.pack(ce.generate(W.spec, 512), world)
+    with engine.forward(wave, world) as tape:
+        g1 = tape.backward()
+        w = np.random.default_rng(3).normal(size=len(wave)).astype(np.float32)
+        gw = tape.backward(w)
+        g0 = tape.backward(np.zeros(len(wave), np.float32))
+    assert (g0 == 0).all()
+    moderate = np.isfinite(g1).all(axis=1) & (np.abs(g1).max(axis=1) < 1e3)
+    assert moderate.mean() > 0.8
+    a, b = gw[moderate], (g1 * w[:, None])[moderate]
+    close = np.abs(a - b) <= 1e-3 * np.abs(b) + 1e-6 * np.abs(b).max()
+    assert close.mean() > 0.999, close.mean()
+
+
+def test_gradients_refuse_unsupported_batches(engine):
+    effects = ce.make_world(duration=1.0, **effects_world_kw())
+    wave = ce.pack(ce.generate(W.spec, 16), effects)
+    with pytest.raises(ce.EngineError) as err:
+        engine.forward(wave, effects)
+    assert err.value.status == ce.CE_ERR_UNSUPPORTED
+    world = W.world(duration=1.0)
+    wave = ce.pack(ce.generate(W.spec, 16), world)
+    sensed = ce.WavePack(wave.lanes, wave.muscles.copy(), wave.heads, wave.slots, wave.info)
+    sensed.muscles.view(np.uint32)[int(wave.heads[0, 4]) + 16] = 0
+    with pytest.raises(ce.EngineError) as err:
+        engine.forward(sensed, world)
+    assert err.value.status == ce.CE_ERR_UNSUPPORTED
+    with pytest.raises(ce.EngineError):
+        engine.forward(wave, world, checkpoint_every=128)

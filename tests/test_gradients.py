@@ -1,0 +1,144 @@
+"""Host-side checks of the gradient path: the gene chain rule and the FP64
+dual-number tangent of the CPU oracle. No GPU is used.
+
+* `ce_gene_gradients` maps record-field gradients (muscle fields, node
+  friction, mass and start position) to gene gradients through the packing
+  arithmetic
+  (src/physics2.rs:190-350, src/physics.rs:203-296, src/kernel.rs:336-411).
+  For random record gradients g and a random gene direction v it must give
+  <g_gene, v> = <g, d records / d genes . v>, the right side taken by central
+  differences of the packer.
+* The oracle's FP64 tangent (forward-mode dual numbers through the restated
+  kernel, shaders/creature.cu:130-742) must equal central differences of the
+  FP64 oracle over trials short enough that the perturbation keeps every
+  contact, friction and joint-limit mode.
+"""
+import numpy as np
+import pytest
+
+import evolution_simulator_gpu_b200 as ce
+from evolution_simulator_gpu_b200.configs import WORKLOADS
+
+# Record float index of each gradient field of a muscle (kernel record layout).
+FIELDS = [8, 3, 4, 5, 10, 11, 12, 13, 14]
+
+
+def _direction(pop, rng):
+    """A gene direction (muscle genes x 5, node genes), zero where the chain
+    rule has a kink: duty at its clamp, phase near its wrap."""
+    vm = rng.normal(size=(len(pop.muscles), 5))
+    vn = rng.normal(size=len(pop.nodes))
+    duty = pop.muscles["duty"]
+    phase = pop.muscles["phase"]
+    bad = (duty <= 0.0501) | (duty >= 0.9499) | (phase < 0.01) | (phase > 0.99)
+    vm[bad, 3:] = 0.0
+    return vm, vn
+
+
+def _moved(pop, vm, vn, h):
+    m = pop.muscles.copy()
+    n = pop.nodes.copy()
+    T = m["period"].astype(np.float64)
+    m["short"] = (m["short"] + h * vm[:, 0]).astype(np.float32)
+    m["long"] = (m["long"] + h * vm[:, 1]).astype(np.float32)
+    m["phase"] = (m["phase"] - h * vm[:, 3] / T).astype(np.float32)
+    m["duty"] = (m["duty"] + h * (vm[:, 4] - vm[:, 3]) / T).astype(np.float32)
+    n["friction"] = (n["friction"] + h * vn).astype(np.float32)
+    strength = None if pop.strength is None else (pop.strength + h * vm[:, 2]).astype(np.float32)
+    return ce.Population(n, pop.bones, m, pop.genomes, strength)
+
+
+def test_gene_chain_rule_matches_packer_differences():
+    w = WORKLOADS["gradients"]
+    world = w.world(duration=1.0)
+    pop = ce.generate(w.spec, 48)
+    assert pop.strength is not None
+    wave = ce.pack(pop, world)
+    rows, mm = int((wave.heads[:, 0] & 255).max()), int(wave.heads[:, 1].max())
+    rng = np.random.default_rng(0)
+    g = rng.normal(size=(len(wave), 9 * mm + 4 * rows)).astype(np.float32)
+    mg, ng = ce.gene_gradients(pop, wave, world, g, (rows, mm))
+    vm, vn = _direction(pop, rng)
+    h = 1e-3
+    wp, wm = ce.pack(_moved(pop, vm, vn, h), world), ce.pack(_moved(pop, vm, vn, -h), world)
+    assert (wp.slots == wave.slots).all() and (wm.slots == wave.slots).all()
+    lhs = 0.0
+    lfp, lfm = wp.lanes.view(np.float32), wm.lanes.view(np.float32)
+    for c in range(len(wave)):
+        M, N = int(wave.heads[c, 1]), int(wave.heads[c, 0] & 255)
+        mo, ro = int(wave.heads[c, 4]), int(wave.heads[c, 3])
+        for k in range(M):
+            for f, fi in enumerate(FIELDS):
+                d = (float(wp.muscles[mo + 20 * k + fi]) - float(wm.muscles[mo + 20 * k + fi])) / (2 * h)
+                lhs += float(g[c, 9 * k + f]) * d
+        for i in range(N):
+            d = (float(lfp[ro + 6 * i + 2]) - float(lfm[ro + 6 * i + 2])) / (2 * h)
+            lhs += float(g[c, 9 * mm + i]) * d
+            d = (float(lfp[ro + 6 * i]) - float(lfm[ro + 6 * i])) / (2 * h)
+            lhs += float(g[c, 9 * mm + rows + i]) * d
+            for axis in range(2):
+                d = (float(lfp[ro + 6 * i + 3 + axis]) - float(lfm[ro + 6 * i + 3 + axis])) / (2 * h)
+                lhs += float(g[c, 9 * mm + 2 * rows + 2 * i + axis]) * d
+    rhs = float((mg * vm).sum() + (ng * vn).sum())
+    assert abs(lhs - rhs) <= 2e-3 * max(abs(rhs), 1.0), (lhs, rhs)
+
+
+@pytest.mark.parametrize("field", range(11))
+def test_fp64_tangent_matches_fp64_differences(field):
+    """One record field of muscle 0 (field < 9), the friction of node 1
+    (field 9) or the mass of node 1 (field 10, with 1 / total mass moving
+    along) of 8 creatures, 0.2 s trials."""
+    from oracle.ref import Oracle
+    o = Oracle()
+    w = WORKLOADS["gradients"]
+    world = w.world(duration=0.2)
+    pop = ce.generate(w.spec, 8)
+    wave = ce.pack(pop, world)
+    p, flags = ce.make_params(world), ce.world_flags(world)
+    rows, mm = 12, 20
+    n = len(wave)
+    dm = np.zeros((n, mm, 9))
+    dn = np.zeros((n, rows))
+    dmass = np.zeros((n, rows))
+    lf = wave.lanes.view(np.float32)
+    for c in range(n):
+        mo, ro = int(wave.heads[c, 4]), int(wave.heads[c, 3])
+        if field < 9:
+            dm[c, 0, field] = wave.muscles[mo + FIELDS[field]]
+        elif field == 9:
+            dn[c, 1] = lf[ro + 6 + 2]
+        else:
+            dmass[c, 1] = lf[ro + 6]
+    tangent, _, _ = o.tangent(wave, p, flags, dm, dn, dmass=dmass)
+
+    def run(eps):
+        mus = wave.muscles.copy()
+        lanes = wave.lanes.copy()
+        heads = wave.heads.copy()
+        lf2 = lanes.view(np.float32)
+        for c in range(n):
+            mo, ro = int(wave.heads[c, 4]), int(wave.heads[c, 3])
+            if field < 9:
+                mus[mo + FIELDS[field]] = np.float32(wave.muscles[mo + FIELDS[field]] * (1 + eps))
+            elif field == 9:
+                lf2[ro + 6 + 2] = np.float32(lf[ro + 6 + 2] * (1 + eps))
+            else:
+                dmass_c = float(lf[ro + 6]) * eps
+                lf2[ro + 6] = np.float32(lf[ro + 6] + dmass_c)
+                inv = np.float32(1.0 / (1.0 / float(np.uint32(wave.heads[c, 6]).view(np.float32)) + dmass_c))
+                heads[c, 6] = inv.view(np.uint32)
+        o.tangent(ce.WavePack(lanes, mus, heads, wave.slots, wave.info), p, flags, np.zeros_like(dm),
+                  np.zeros_like(dn))
+        return o.fitness64.copy()
+
+    h = 1e-3
+    f0, fp, fm = run(0.0), run(h), run(-h)
+    fd = (fp - fm) / (2 * h)
+    # Mode-preserving perturbations only: the one-sided differences agree
+    # (a perturbation that crosses a contact, friction, joint-limit or rhythm
+    # branch shows as a jump between them).
+    up, down = (fp - f0) / h, (f0 - fm) / h
+    keep = np.abs(up - down) <= 0.05 * np.maximum(np.abs(up), np.abs(down)) + 1e-9
+    assert keep.sum() >= n // 2, keep
+    scale = max(np.abs(fd[keep]).max(), 1e-9)
+    assert np.allclose(tangent[keep], fd[keep], rtol=2e-2, atol=2e-2 * scale), (tangent, fd, keep)
