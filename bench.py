@@ -228,7 +228,7 @@ def gradient_workload():
     from evolution_simulator_gpu_b200.configs import WORKLOADS
     w = WORKLOADS["gradients"]
     world = w.world()
-    pop = ce.generate(w.spec, w.creatures)
+    pop = ce.generate(w.spec, w.count)
     wave = ce.pack(pop, world)
     params = 5 * wave.heads[:, 1].astype(np.int64).sum() + (wave.heads[:, 0] & 255).astype(np.int64).sum()
     return world, pop, wave, float(params) / len(wave)
