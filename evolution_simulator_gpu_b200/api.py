@@ -176,6 +176,16 @@ def _bind(lib: C.CDLL) -> None:
         "ce_to_metrics_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
         "ce_forward": (C.c_int, [C.c_void_p, P(WavePackC), P(World), C.c_uint32, P(C.c_void_p)]),
+        "ce_graph_open": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(World), P(C.c_void_p)]),
+        "ce_graph_launch": (C.c_int, [C.c_void_p, P(C.c_double)]),
+        "ce_graph_results": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),
+        "ce_graph_close": (C.c_int, [C.c_void_p]),
+        "ce_metrics_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_shape_classes": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
+        "ce_height_bin_edges": (None, [C.c_void_p]),
+        "ce_replay_decode": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_tape_results": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
         "ce_tape_grad_floats": (C.c_uint32, [C.c_void_p]),
         "ce_tape_shape": (C.c_int, [C.c_void_p, P(C.c_uint32), P(C.c_uint32)]),
@@ -209,7 +219,9 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
-            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints"]
+            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
+            "ce_replay_decode", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
+            "ce_graph_launch", "ce_graph_results", "ce_graph_close"]
 
 
 def _check(status: int, what: str) -> None:
@@ -565,6 +577,70 @@ class Engine:
                "ce_advance_device")
 
 
+# ------------------------------------------------------------------ graphs
+class GenerationGraph:
+    """Several packed generations resident on the device and run as one CUDA
+    graph (ce_graph_open): `launch()` runs them all and returns the GPU
+    seconds; `results(k)` reads generation k's results (packed order)."""
+
+    def __init__(self, engine: "Engine", waves, world: World):
+        self._waves = list(waves)  # the packs stay alive while the graph is open
+        arr = (WavePackC * len(self._waves))(*[w.c() for w in self._waves])
+        h = C.c_void_p()
+        _check(lib().ce_graph_open(engine.handle, arr, len(self._waves), C.byref(world), C.byref(h)), "ce_graph_open")
+        self._h = h
+
+    def launch(self) -> float:
+        secs = C.c_double()
+        _check(lib().ce_graph_launch(self._h, C.byref(secs)), "ce_graph_launch")
+        return secs.value
+
+    def results(self, k: int) -> np.ndarray:
+        out = np.zeros(len(self._waves[k]), RESULT_DTYPE)
+        _check(lib().ce_graph_results(self._h, k, _ptr(out), len(out)), "ce_graph_results")
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().ce_graph_close(self._h)
+            self._h = None
+
+    def __enter__(self) -> "GenerationGraph":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ replay
+def replay_decode(bones: np.ndarray, muscles: int, frames: np.ndarray) -> dict:
+    """One recorded creature's frames [frame, slot, 2] (Engine.record) in its
+    own node numbering (engine::recorded, src/engine.rs:1062-1127):
+    positions [frame, node, 2] and, when the frames carry them, energy and
+    pull [frame, muscle], ground and friction [frame, node], broken [frame]."""
+    bones = np.ascontiguousarray(bones, BONE_DTYPE)
+    nodes = len(bones) + 1
+    fr = np.ascontiguousarray(frames, np.float32)
+    count, stride = fr.shape[0], fr.shape[1]
+    out = {"positions": np.zeros((count, nodes, 2), np.float32)}
+    forces = stride > MAX_NODES + muscles + nodes
+    if forces:
+        out.update(energy=np.zeros((count, muscles), np.float32), pull=np.zeros((count, muscles), np.float32),
+                   ground=np.zeros((count, nodes), np.float32), friction=np.zeros((count, nodes), np.float32),
+                   broken=np.zeros(count, np.uint64))
+    g = out.get
+    _check(lib().ce_replay_decode(_ptr(bones), nodes, muscles, _ptr(fr), count, stride, _ptr(out["positions"]),
+                                  _ptr(g("energy")), _ptr(g("pull")), _ptr(g("ground")), _ptr(g("friction")),
+                                  _ptr(g("broken"))), "ce_replay_decode")
+    return out
+
+
 # ---------------------------------------------------------------- gradients
 GRAD_MUSCLE_FIELDS = ["amplitude", "hill", "cap", "inv_capacity", "phase", "duty", "inv_duty", "inv_complement",
                       "stiffness"]
@@ -705,6 +781,33 @@ def niche_cells(pop: Population, metrics: np.ndarray, indices=None, global_layou
     _check(lib().ce_niche_batch(C.byref(pc), _ptr(idx), n, m.ctypes.data, 1 if global_layout else 0,
                                 cells.ctypes.data), "ce_niche_batch")
     return cells
+
+
+def shape_classes(pop: Population, wave: "WavePack", indices=None, global_layout: bool = True) -> np.ndarray:
+    """The niche's shape class (aspect axis) of each packed creature, for
+    metrics_device."""
+    out = np.zeros(len(wave), np.uint8)
+    idx = None if indices is None else np.ascontiguousarray(indices, np.uint32)
+    pc = pop.c()
+    _check(lib().ce_shape_classes(C.byref(pc), _ptr(idx), len(wave), _ptr(wave.slots), 1 if global_layout else 0,
+                                  _ptr(out)), "ce_shape_classes")
+    return out
+
+
+def height_bin_edges() -> np.ndarray:
+    """The mean heights where the niche's height bin steps up."""
+    out = np.zeros(5, np.float32)
+    lib().ce_height_bin_edges(_ptr(out))
+    return out
+
+
+def metrics_device(results: int, heads: int, shapes: int, count: int, world: World, metrics: int, cells: int,
+                   stream: int = 0, global_layout: bool = True) -> None:
+    """The metrics epilogue on device pointers (asynchronous on `stream`):
+    metrics rows (METRICS_DTYPE, `metrics` 0 to skip) and dense cells (int64)
+    of `count` results, equal to to_metrics and niche_cells to the bit."""
+    _check(lib().ce_metrics_device(results, heads, shapes, count, C.byref(world), 1 if global_layout else 0,
+                                   metrics or None, cells, stream or None), "ce_metrics_device")
 
 
 def ground(x: float, amplitude: float = 0.0, tilt: float = 0.0, width: float = 0.0, hurdle: float = 0.0,

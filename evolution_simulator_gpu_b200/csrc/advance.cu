@@ -75,6 +75,25 @@ cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_pa
     return cudaErrorInvalidValue;
 }
 
+cudaError_t advance_reserve_smem(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block) {
+    const int smem = (int)smem_bytes(rows, mm, block);
+    auto go = [&](auto rec_tag, auto rate_tag) -> cudaError_t {
+        constexpr bool R = decltype(rec_tag)::value;
+        constexpr int RT = decltype(rate_tag)::value;
+        return by_world<R, RT>(flags, [&](auto w) {
+            return cudaFuncSetAttribute(advance_kernel<decltype(w), R, RT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        });
+    };
+    using Tt = std::true_type;
+    using Ft = std::false_type;
+    using R60 = std::integral_constant<int, 60>;
+    using R120 = std::integral_constant<int, 120>;
+    if (rate == 60) return record ? go(Tt{}, R60{}) : go(Ft{}, R60{});
+    if (rate == 120) return record ? go(Tt{}, R120{}) : go(Ft{}, R120{});
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block,
                               int* blocks) {
     auto go = [&](auto rec_tag, auto rate_tag) -> cudaError_t {

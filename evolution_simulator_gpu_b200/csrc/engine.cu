@@ -850,3 +850,198 @@ extern "C" ce_status ce_tape_checkpoints(ce_tape* t, float* out, size_t cap_floa
     if (per_creature) *per_creature = t->ckpts;
     return CE_OK;
 }
+
+// ------------------------------------------------------ generation graphs
+// Several packed generations run as one CUDA graph: per generation the
+// node-count bucketing and the size classes' launches (two streams joined
+// by events), the generations one after another, all captured once and
+// replayed by ce_graph_launch. Batches stay resident on the device.
+struct ce_graph {
+    ce_engine* engine = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr;
+    std::vector<cudaEvent_t> events;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct Gen {
+        DeviceBuf lanes, muscles, heads, buckets, results;
+        size_t count = 0;
+    };
+    std::vector<Gen> gens;
+    std::vector<DeviceBuf> scratch;  // one a size class, shared by the generations
+};
+
+extern "C" ce_status ce_graph_close(ce_graph* g) {
+    if (!g) return CE_OK;
+    if (g->engine) cudaSetDevice(g->engine->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    for (auto& gen : g->gens) {
+        for (DeviceBuf* b : {&gen.lanes, &gen.muscles, &gen.heads, &gen.buckets, &gen.results}) b->release();
+    }
+    for (auto& b : g->scratch) b.release();
+    for (cudaEvent_t ev : g->events) cudaEventDestroy(ev);
+    if (g->start) cudaEventDestroy(g->start);
+    if (g->stop) cudaEventDestroy(g->stop);
+    if (g->side) cudaStreamDestroy(g->side);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint32_t generations, const ce_world* w,
+                                   ce_graph** out) {
+    if (!e || !packs || !out || generations == 0) {
+        set_error("ce_graph_open: null argument or no generation");
+        return CE_ERR_INVALID;
+    }
+    *out = nullptr;
+    ce_status s = check_world(w);
+    if (s != CE_OK) return s;
+    ce_graph* g = new ce_graph;
+    g->engine = e;
+    auto fail = [&](ce_status st) {
+        ce_graph_close(g);
+        return st;
+    };
+    if ((s = set_device(e)) != CE_OK) return fail(s);
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (s = cuda_status(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (s = cuda_status(cudaEventCreate(&g->start), "cudaEventCreate")) ||
+        (s = cuda_status(cudaEventCreate(&g->stop), "cudaEventCreate"))) {
+        return fail(s);
+    }
+    const uint32_t flags = ce_world_flags(w);
+    const int rate = (int)ce::world_rate(*w);
+    ce_params p;
+    // Plans, grids and scratch of every generation; one scratch a class.
+    std::vector<std::vector<ClassPlan>> plans(generations);
+    std::vector<std::vector<unsigned>> grids(generations);
+    size_t scratch_need[2] = {0, 0};
+    g->gens.resize(generations);
+    for (uint32_t k = 0; k < generations; k++) {
+        const ce_wave_pack* pack = packs + k;
+        if (!pack->count) {
+            set_error("ce_graph_open: empty generation");
+            return fail(CE_ERR_INVALID);
+        }
+        if ((s = plan_classes(pack, plans[k])) != CE_OK) return fail(s);
+        for (const ClassPlan& c : plans[k]) {
+            const unsigned grid = grid_for(e, c.rows, c.mm, flags, false, rate, c.count);
+            grids[k].push_back(grid);
+            const size_t at = grids[k].size() - 1;
+            scratch_need[at] = std::max(scratch_need[at], scratch_bytes(grid, c.rows, c.mm, false));
+        }
+        ce_graph::Gen& gen = g->gens[k];
+        gen.count = pack->count;
+        const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
+        if ((s = gen.lanes.ensure(lanes_b)) || (s = gen.muscles.ensure(std::max<size_t>(mus_b, 4))) ||
+            (s = gen.heads.ensure(heads_b)) || (s = gen.buckets.ensure(cek::bucket_bytes(pack->count))) ||
+            (s = gen.results.ensure(pack->count * sizeof(ce_result)))) {
+            return fail(s);
+        }
+        if ((s = cuda_status(cudaMemcpy(gen.lanes.ptr, pack->lanes, lanes_b, cudaMemcpyHostToDevice), "cudaMemcpy")) ||
+            (s = cuda_status(cudaMemcpy(gen.muscles.ptr, pack->muscles, mus_b, cudaMemcpyHostToDevice), "cudaMemcpy")) ||
+            (s = cuda_status(cudaMemcpy(gen.heads.ptr, pack->heads, heads_b, cudaMemcpyHostToDevice), "cudaMemcpy"))) {
+            return fail(s);
+        }
+    }
+    g->scratch.resize(2);
+    for (int c = 0; c < 2; c++) {
+        if (scratch_need[c] && (s = g->scratch[c].ensure(scratch_need[c])) != CE_OK) return fail(s);
+    }
+    g->events.resize(2 * generations, nullptr);
+    for (auto& ev : g->events) {
+        if ((s = cuda_status(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate"))) return fail(s);
+    }
+    // Kernel attributes are set by the occupancy queries above, before the
+    // capture; the capture itself holds only stream work.
+    if ((s = cuda_status(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture")))
+        return fail(s);
+    ce_status cap = CE_OK;
+    for (uint32_t k = 0; k < generations && cap == CE_OK; k++) {
+        ce_graph::Gen& gen = g->gens[k];
+        ce_make_params(w, 0, (uint32_t)gen.count, 0, &p);
+        const cek::Buckets bk = cek::bucket_layout(gen.buckets.ptr, gen.count);
+        cap = cuda_status(cek::launch_bucket(static_cast<const uint4*>(gen.heads.ptr), 0u, (uint32_t)gen.count, bk,
+                                             g->stream),
+                          "bucketing launch");
+        if (cap == CE_OK) cap = cuda_status(cudaEventRecord(g->events[2 * k], g->stream), "cudaEventRecord");
+        if (cap == CE_OK) cap = cuda_status(cudaStreamWaitEvent(g->side, g->events[2 * k], 0), "cudaStreamWaitEvent");
+        for (size_t c = 0; c < plans[k].size() && cap == CE_OK; c++) {
+            cek::KernelArgs a{};
+            a.records = static_cast<const uint32_t*>(gen.lanes.ptr);
+            a.muscles = static_cast<const float*>(gen.muscles.ptr);
+            a.heads = static_cast<const uint4*>(gen.heads.ptr);
+            a.results = static_cast<ce_result*>(gen.results.ptr);
+            a.counter = bk.counters + plans[k][c].first_n;
+            a.scratch = static_cast<float4*>(g->scratch[c].ptr);
+            a.order = bk.order;
+            a.bounds = bk.bounds + plans[k][c].first_n;
+            a.work = bk.work + plans[k][c].first_n;
+            a.queues = plans[k][c].last_n - plans[k][c].first_n + 1u;
+            a.count = plans[k][c].count;
+            a.rows = plans[k][c].rows;
+            a.mm = plans[k][c].mm;
+            a.chunk_k = e->chunk_k;
+            cek::LaunchSpec ls{plans[k][c].rows, plans[k][c].mm, flags, false, rate, grids[k][c], cek::kBlock,
+                               c == 0 ? g->stream : g->side};
+            cap = cuda_status(cek::launch_advance(ls, a, p), "advance launch");
+        }
+        if (cap == CE_OK) cap = cuda_status(cudaEventRecord(g->events[2 * k + 1], g->side), "cudaEventRecord");
+        if (cap == CE_OK) cap = cuda_status(cudaStreamWaitEvent(g->stream, g->events[2 * k + 1], 0), "cudaStreamWaitEvent");
+    }
+    cudaGraph_t graph = nullptr;
+    const ce_status end = cuda_status(cudaStreamEndCapture(g->stream, &graph), "cudaStreamEndCapture");
+    g->graph = graph;
+    if (cap != CE_OK) return fail(cap);
+    if (end != CE_OK) return fail(end);
+    // The largest tables of any launch in the graph.
+    unsigned max_rows = 2, max_mm = 0;
+    size_t max_smem = 0;
+    for (const auto& ps : plans) {
+        for (const ClassPlan& c : ps) {
+            const size_t b = cek::smem_bytes(c.rows, c.mm, cek::kBlock);
+            if (b > max_smem) {
+                max_smem = b;
+                max_rows = c.rows;
+                max_mm = c.mm;
+            }
+        }
+    }
+    if ((s = cuda_status(cek::advance_reserve_smem(max_rows, max_mm, flags, false, rate, cek::kBlock),
+                         "cudaFuncSetAttribute")) ||
+        (s = cuda_status(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate"))) {
+        return fail(s);
+    }
+    *out = g;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_graph_launch(ce_graph* g, double* seconds) {
+    if (!g || !g->exec) return CE_ERR_INVALID;
+    ce_status s = set_device(g->engine);
+    if (s != CE_OK) return s;
+    CE_TRY(cudaEventRecord(g->start, g->stream), "cudaEventRecord");
+    CE_TRY(cudaGraphLaunch(g->exec, g->stream), "cudaGraphLaunch");
+    CE_TRY(cudaEventRecord(g->stop, g->stream), "cudaEventRecord");
+    CE_TRY(cudaEventSynchronize(g->stop), "generation graph");
+    float ms = 0.0f;
+    CE_TRY(cudaEventElapsedTime(&ms, g->start, g->stop), "cudaEventElapsedTime");
+    if (seconds) *seconds = ms * 1e-3;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_graph_results(ce_graph* g, uint32_t generation, ce_result* out, size_t cap) {
+    if (!g || !out || generation >= g->gens.size() || cap < g->gens[generation].count) {
+        set_error("ce_graph_results: bad generation or buffer too small");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = set_device(g->engine);
+    if (s != CE_OK) return s;
+    CE_TRY(cudaMemcpy(out, g->gens[generation].results.ptr, g->gens[generation].count * sizeof(ce_result),
+                      cudaMemcpyDeviceToHost),
+           "cudaMemcpy");
+    return CE_OK;
+}

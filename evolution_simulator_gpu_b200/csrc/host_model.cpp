@@ -828,10 +828,9 @@ static float height_axis(float h) {
     return clampf(std::log(fmax_(h, low) / low) / std::log(high / low), 0.0f, 1.0f);
 }
 
-extern "C" int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint32_t muscle_count,
-                            const ce_metrics* m, int global_layout, uint8_t niche_out[6]) {
-    (void)muscle_count;
-    if (!nodes || !m) return -1;
+// The shape class of a body (qd.rs:762-790): its gene extent's aspect
+// against the layout's edges.
+static uint8_t shape_class(const ce_node_gene* nodes, uint32_t node_count, int global_layout) {
     float min_x = std::numeric_limits<float>::infinity(), max_x = -min_x;
     float min_y = min_x, max_y = -min_x;
     for (uint32_t i = 0; i < node_count; i++) {
@@ -840,21 +839,31 @@ extern "C" int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint
         min_y = fmin_(min_y, nodes[i].y);
         max_y = fmax_(max_y, nodes[i].y);
     }
+    const float aspect = clampf(fmax_(max_x - min_x, 0.01f) / fmax_(max_y - min_y, 0.01f), 0.0625f, 16.0f);
+    static const float g_aspect[3] = {0.9f, 1.4f, 2.5f};
+    static const float i_aspect[2] = {1.2f, 2.0f};
+    const float* ae = global_layout ? g_aspect : i_aspect;
+    const int edges = global_layout ? 3 : 2;
+    uint8_t shape = 0;
+    for (int e = 0; e < edges; e++) shape += aspect >= ae[e] ? 1 : 0;
+    return shape;
+}
+
+extern "C" int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint32_t muscle_count,
+                            const ce_metrics* m, int global_layout, uint8_t niche_out[6]) {
+    (void)muscle_count;
+    if (!nodes || !m) return -1;
     const float gc = clampf(m->ground_contact, 0.0f, 1.0f);
     const float gf = clampf(m->gait_frequency, 0.0f, 20.0f);
-    const float aspect = clampf(fmax_(max_x - min_x, 0.01f) / fmax_(max_y - min_y, 0.01f), 0.0625f, 16.0f);
     const float mh = fmax_(m->mean_height, 0.0f);
     const float feet = fmax_(m->feet, 0.0f);
-    static const float g_aspect[3] = {0.9f, 1.4f, 2.5f};
     static const uint16_t g_nodes[3] = {9, 11, 14};
-    static const float i_aspect[2] = {1.2f, 2.0f};
     static const uint16_t i_nodes[2] = {9, 12};
-    const float* ae = global_layout ? g_aspect : i_aspect;
     const uint16_t* ne = global_layout ? g_nodes : i_nodes;
     const int edges = global_layout ? 3 : 2;
-    uint8_t shape = 0, size = 0;
+    const uint8_t shape = shape_class(nodes, node_count, global_layout);
+    uint8_t size = 0;
     for (int e = 0; e < edges; e++) {
-        shape += aspect >= ae[e] ? 1 : 0;
         size += (uint16_t)node_count >= ne[e] ? 1 : 0;
     }
     const float fr = std::round(feet);
@@ -1029,3 +1038,109 @@ extern "C" ce_status ce_gene_gradients(const ce_population* pop, const uint32_t*
     }
     return CE_OK;
 }
+
+// ------------------------------------------------------------------ replay
+// engine::recorded (src/engine.rs:1062-1127): the frames of one recorded
+// creature (ce_record's layout, `stride` float2 slots a frame, kernel node
+// rows first) in the creature's own node numbering (row 0 is node 0, row
+// j + 1 is bone j's far node), and, when the frames carry them, the forces:
+// each muscle's energy store and pull, each node's ground and friction force,
+// and the broken-joint bits.
+extern "C" ce_status ce_replay_decode(const ce_bone_gene* bones, uint32_t node_count, uint32_t muscles,
+                                      const float* frames, uint32_t count, uint32_t stride, float* positions,
+                                      float* energy, float* pull, float* ground, float* friction,
+                                      uint64_t* broken) {
+    if (!bones || !frames || !positions || node_count < 1 || node_count > CE_MAX_NODES) {
+        set_error("ce_replay_decode: null argument or bad node count");
+        return CE_ERR_INVALID;
+    }
+    if (stride < node_count) {
+        set_error("ce_replay_decode: frames narrower than the body");
+        return CE_ERR_INVALID;
+    }
+    std::vector<uint32_t> order(node_count);
+    order[0] = 0;
+    for (uint32_t j = 0; j + 1 < node_count; j++) {
+        if (bones[j].b >= node_count) {
+            set_error("ce_replay_decode: bone end outside the body");
+            return CE_ERR_INVALID;
+        }
+        order[j + 1] = bones[j].b;
+    }
+    const uint32_t capacity = CE_MAX_NODES;
+    const bool forces = stride > capacity + muscles + node_count;
+    if ((energy || pull || ground || friction || broken) && !forces) {
+        set_error("ce_replay_decode: the frames carry no forces");
+        return CE_ERR_INVALID;
+    }
+    for (uint32_t t = 0; t < count; t++) {
+        const float* f = frames + (size_t)t * stride * 2;
+        for (uint32_t k = 0; k < node_count; k++) {
+            positions[((size_t)t * node_count + order[k]) * 2] = f[2 * k];
+            positions[((size_t)t * node_count + order[k]) * 2 + 1] = f[2 * k + 1];
+        }
+        if (!forces) continue;
+        const float* slot = f + 2 * capacity;
+        for (uint32_t m = 0; m < muscles; m++) {
+            if (energy) energy[(size_t)t * muscles + m] = slot[2 * m];
+            if (pull) pull[(size_t)t * muscles + m] = slot[2 * m + 1];
+        }
+        for (uint32_t k = 0; k < node_count; k++) {
+            if (ground) ground[(size_t)t * node_count + order[k]] = slot[2 * (muscles + k)];
+            if (friction) friction[(size_t)t * node_count + order[k]] = slot[2 * (muscles + k) + 1];
+        }
+        if (broken) {
+            uint32_t lo, hi;
+            std::memcpy(&lo, f + 2 * (stride - 1), 4);
+            std::memcpy(&hi, f + 2 * (stride - 1) + 1, 4);
+            broken[t] = (uint64_t)lo | ((uint64_t)hi << 32);
+        }
+    }
+    return CE_OK;
+}
+
+// --------------------------------------------------- metrics on the device
+// Shape classes of a packed batch (packed order), for the device epilogue.
+extern "C" ce_status ce_shape_classes(const ce_population* pop, const uint32_t* indices, size_t n,
+                                      const uint32_t* slots, int global_layout, uint8_t* out) {
+    if (!pop || !slots || !out) {
+        set_error("ce_shape_classes: null argument");
+        return CE_ERR_INVALID;
+    }
+    for (size_t c = 0; c < n; c++) {
+        const size_t i = indices ? indices[slots[c]] : slots[c];
+        const ce_genome& g = pop->genomes[i];
+        out[c] = shape_class(pop->nodes + g.node_start, g.node_count, global_layout);
+    }
+    return CE_OK;
+}
+
+namespace ce {
+// The mean heights where the niche's height bin steps up: bin(h) is the
+// number of thresholds at or below h. The bin is monotone in h, so the
+// smallest float reaching each bin, found by bisection over the float bits
+// with the host's own arithmetic, reproduces it exactly.
+void height_bin_thresholds(float out[5]) {
+    auto bin = [](float h) { return qd_bin(height_axis(fmax_(h, 0.0f)), 0.0f, 1.0f, 6); };
+    const uint32_t inf_bits = 0x7f800000u;
+    for (int b = 1; b <= 5; b++) {
+        uint32_t lo = 0, hi = inf_bits;  // bin(lo) < b <= bin(hi), or none
+        float v;
+        if (bin(std::numeric_limits<float>::max()) < b) {
+            out[b - 1] = std::numeric_limits<float>::infinity();
+            continue;
+        }
+        hi = 0x7f7fffffu;
+        if (bin(0.0f) >= b) {
+            out[b - 1] = 0.0f;
+            continue;
+        }
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            std::memcpy(&v, &mid, 4);
+            if (bin(v) >= b) hi = mid; else lo = mid;
+        }
+        std::memcpy(&out[b - 1], &hi, 4);
+    }
+}
+}  // namespace ce

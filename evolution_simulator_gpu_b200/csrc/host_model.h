@@ -27,4 +27,7 @@ uint32_t world_settle(const ce_world& w);
 uint32_t world_sample(const ce_world& w);
 uint32_t world_steps(const ce_world& w);
 float world_air_per_step(const ce_world& w);
+// The mean heights where the niche's height bin steps up (metrics epilogue).
+void height_bin_thresholds(float out[5]);
+
 }  // namespace ce

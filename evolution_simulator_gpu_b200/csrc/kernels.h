@@ -119,5 +119,8 @@ unsigned slot_lines(unsigned rows, unsigned mm, bool record);
 cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
 cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block,
                               int* blocks);
+// Sets the kernel's dynamic shared-memory limit for `rows` x `mm` tables: a
+// CUDA graph's launches are checked against the limit in force when it runs.
+cudaError_t advance_reserve_smem(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block);
 
 }  // namespace cek

@@ -202,6 +202,16 @@ void ce_ground(float x, float amplitude, float tilt, float width, float hurdle, 
 /* The quake hash of a creature id (physics::quake_hash, src/physics.rs:640-648). */
 uint32_t ce_quake_hash(uint64_t id);
 
+/* One recorded creature's frames (count frames of `stride` float2 slots, as
+ * ce_record writes them) in the creature's own node numbering
+ * (engine::recorded, src/engine.rs:1062-1127): positions[count][nodes][2];
+ * with forces in the frames, energy[count][muscles], pull[count][muscles],
+ * ground[count][nodes], friction[count][nodes] and broken[count] (each NULL
+ * to skip). `bones` are the creature's bone genes in canonical order. */
+ce_status ce_replay_decode(const ce_bone_gene* bones, uint32_t node_count, uint32_t muscles,
+                           const float* frames, uint32_t count, uint32_t stride, float* positions,
+                           float* energy, float* pull, float* ground, float* friction, uint64_t* broken);
+
 /* Frame slots of a recording (src/creature_kernel.rs:312-326). */
 uint32_t ce_frame_stride(uint32_t max_muscles);
 
@@ -235,6 +245,22 @@ typedef struct ce_metrics {
     float screen_x;
     uint32_t screened, steps;
 } ce_metrics;
+
+/* The metrics epilogue on the device: ce_to_metrics and the dense cell of
+ * ce_niche for `count` results (device pointers: results, heads of the
+ * packed batch, shape classes from ce_shape_classes; `metrics` may be NULL),
+ * equal to the host's to the bit; asynchronous on `stream` (a cudaStream_t).
+ * No counterpart in the reference, which does this on the host
+ * (src/scheduler.rs:890-923, src/qd.rs:762-999). */
+ce_status ce_metrics_device(const ce_result* results, const uint32_t* heads, const uint8_t* shape_classes,
+                            size_t count, const ce_world* world, int global_layout, ce_metrics* metrics,
+                            int64_t* cells, void* stream);
+/* Shape classes (the niche's aspect axis, from the genes) of a batch packed
+ * by ce_pack(pop, indices, n, ..., slots, ...), in packed order. */
+ce_status ce_shape_classes(const ce_population* pop, const uint32_t* indices, size_t n, const uint32_t* slots,
+                           int global_layout, uint8_t* out);
+/* The five mean heights where the niche's height bin steps up. */
+void ce_height_bin_edges(float out[5]);
 
 /* scheduler::to_metrics for one result (src/scheduler.rs:859-923). */
 ce_status ce_to_metrics(const ce_result* r, uint32_t node_count, const ce_world* world,
@@ -303,6 +329,20 @@ ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const fl
                             void* scratch, const ce_params* params, uint32_t world_flags,
                             uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
                             void* stream);
+
+/* Several generations as one CUDA graph (no counterpart in the reference,
+ * which launches each wave): the packed batches are copied to the device
+ * once; ce_graph_launch runs every generation (node-count bucketing and the
+ * size classes' launches, generation after generation) as one graph launch
+ * and gives its GPU seconds; ce_graph_results reads a generation's results in
+ * packed order. Kernel attributes are set while opening, so the capture holds
+ * stream work only. */
+typedef struct ce_graph ce_graph;
+ce_status ce_graph_open(ce_engine* engine, const ce_wave_pack* packs, uint32_t generations,
+                        const ce_world* world, ce_graph** graph);
+ce_status ce_graph_launch(ce_graph* graph, double* seconds);
+ce_status ce_graph_results(ce_graph* graph, uint32_t generation, ce_result* out, size_t cap);
+ce_status ce_graph_close(ce_graph* graph);
 
 /* Gradients of fitness (no counterpart in the reference, which has no
  * derivatives): a forward/backward pair shaped like an autograd function.
