@@ -127,7 +127,7 @@ class GenSpec(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("warps_per_cta", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("chunk_k", C.c_uint32), ("small_body", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 # --------------------------------------------------------------- library
@@ -177,6 +177,7 @@ def _bind(lib: C.CDLL) -> None:
         "ce_niche_batch": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
         "ce_forward": (C.c_int, [C.c_void_p, P(WavePackC), P(World), C.c_uint32, P(C.c_void_p)]),
         "ce_graph_open": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(World), P(C.c_void_p)]),
+        "ce_autotune": (C.c_int, [C.c_void_p, P(WavePackC), P(World), P(Options), P(C.c_double)]),
         "ce_graph_launch": (C.c_int, [C.c_void_p, P(C.c_double)]),
         "ce_graph_results": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),
         "ce_graph_close": (C.c_int, [C.c_void_p]),
@@ -221,7 +222,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
             "ce_replay_decode", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
-            "ce_graph_launch", "ce_graph_results", "ce_graph_close"]
+            "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
 
 
 def _check(status: int, what: str) -> None:
@@ -459,12 +460,26 @@ def frame_stride(max_muscles: int) -> int:
 class Engine:
     """One GPU's engine (the reference's ThreadedEngine surface)."""
 
-    def __init__(self, device: int = 0, slots: int = 0, ctas_per_sm: int = 0):
+    def __init__(self, device: int = 0, slots: int = 0, ctas_per_sm: int = 0, chunk_k: int = 0,
+                 small_body: int = 0):
+        """`ctas_per_sm` (0: as many as fit), `chunk_k` (creatures a warp
+        claims per queue visit, 0: 4) and `small_body` (largest node count run
+        as a small body, 0: 16) are the launch shape; `autotune` picks them."""
         h = C.c_void_p()
-        opts = Options(slots, ctas_per_sm, 0)
+        opts = Options(slots, ctas_per_sm, 0, chunk_k, small_body)
         _check(lib().ce_open(device, C.byref(opts), C.byref(h)), "ce_open")
         self._h = h
         self.device = device
+
+    def autotune(self, sample: WavePack, world: World) -> tuple[dict, float]:
+        """Time `sample` under each launch shape (CTAs per SM x claim chunk x
+        small-body bound) and keep the fastest for later submissions:
+        ({ctas_per_sm, chunk_k, small_body}, its GPU-busy seconds). Results do
+        not depend on the launch shape."""
+        best, secs = Options(), C.c_double()
+        _check(lib().ce_autotune(self.handle, C.byref(sample.c()), C.byref(world), C.byref(best), C.byref(secs)),
+               "ce_autotune")
+        return {"ctas_per_sm": best.ctas_per_sm, "chunk_k": best.chunk_k, "small_body": best.small_body}, secs.value
 
     @property
     def handle(self) -> C.c_void_p:

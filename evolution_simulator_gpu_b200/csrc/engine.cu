@@ -28,7 +28,7 @@ using ce::set_error;
 
 namespace {
 
-// Bodies of up to this many nodes form the first size class.
+// Bodies of up to this many nodes form the first size class (default).
 constexpr unsigned kSmallBody = 16u;
 
 ce_status cuda_status(cudaError_t e, const char* what) {
@@ -111,6 +111,7 @@ struct ce_engine {
     int sms = 0;
     unsigned ctas_per_sm = 0;  // 0: from the occupancy of each kernel
     unsigned chunk_k = 4;
+    unsigned small_body = kSmallBody;
     std::vector<Slot> slots;
     std::deque<size_t> pending;  // slot indices, oldest first
     uint64_t next_ticket = 1;
@@ -165,7 +166,7 @@ ce_status check_world(const ce_world* w) {
 // kSmallBody nodes, and larger ones). Each class runs as one launch whose
 // claim queues are its node counts (kernels.h); the bucketing kernels build
 // the queues on the device.
-ce_status plan_classes(const ce_wave_pack* pack, std::vector<ClassPlan>& plans) {
+ce_status plan_classes(const ce_wave_pack* pack, std::vector<ClassPlan>& plans, unsigned small_body = kSmallBody) {
     plans.clear();
     size_t per_n[CE_MAX_NODES + 1] = {};
     uint32_t mm_n[CE_MAX_NODES + 1] = {};
@@ -183,7 +184,7 @@ ce_status plan_classes(const ce_wave_pack* pack, std::vector<ClassPlan>& plans) 
     for (int big = 0; big < 2; big++) {
         ClassPlan c{0, 0, 0, 2, 0};
         for (unsigned n = 2; n <= CE_MAX_NODES; n++) {
-            if (per_n[n] == 0 || (n > kSmallBody) != (big != 0)) continue;
+            if (per_n[n] == 0 || (n > small_body) != (big != 0)) continue;
             if (c.count == 0) c.first_n = n;
             c.last_n = n;
             c.count += (uint32_t)per_n[n];
@@ -224,6 +225,8 @@ extern "C" ce_status ce_open(int device, const ce_options* options, ce_engine** 
     if (options) {
         if (options->slots) nslots = options->slots;
         e->ctas_per_sm = options->ctas_per_sm;
+        if (options->chunk_k) e->chunk_k = options->chunk_k;
+        if (options->small_body) e->small_body = std::min<unsigned>(options->small_body, CE_MAX_NODES);
     }
     ce_status s = set_device(e);
     if (s != CE_OK) {
@@ -351,7 +354,7 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     Slot& sl = e->slots[si];
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
     std::vector<ClassPlan> plans;
-    if ((s = plan_classes(pack, plans)) != CE_OK) return s;
+    if ((s = plan_classes(pack, plans, e->small_body)) != CE_OK) return s;
     const uint32_t flags = ce_world_flags(w);
     const int rate = (int)ce::world_rate(*w);
     ce_params p;
@@ -926,7 +929,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
             set_error("ce_graph_open: empty generation");
             return fail(CE_ERR_INVALID);
         }
-        if ((s = plan_classes(pack, plans[k])) != CE_OK) return fail(s);
+        if ((s = plan_classes(pack, plans[k], e->small_body)) != CE_OK) return fail(s);
         for (const ClassPlan& c : plans[k]) {
             const unsigned grid = grid_for(e, c.rows, c.mm, flags, false, rate, c.count);
             grids[k].push_back(grid);
@@ -1043,5 +1046,61 @@ extern "C" ce_status ce_graph_results(ce_graph* g, uint32_t generation, ce_resul
     CE_TRY(cudaMemcpy(out, g->gens[generation].results.ptr, g->gens[generation].count * sizeof(ce_result),
                       cudaMemcpyDeviceToHost),
            "cudaMemcpy");
+    return CE_OK;
+}
+
+extern "C" ce_status ce_autotune(ce_engine* e, const ce_wave_pack* sample, const ce_world* w, ce_options* best,
+                                 double* seconds) {
+    if (!e || !sample || !sample->count) {
+        set_error("ce_autotune: null argument or empty sample");
+        return CE_ERR_INVALID;
+    }
+    const unsigned keep_cta = e->ctas_per_sm, keep_chunk = e->chunk_k, keep_small = e->small_body;
+    std::vector<ce_result> out(sample->count);
+    auto time_one = [&](double* busy) -> ce_status {
+        uint64_t ticket = 0, got = 0;
+        ce_status s = ce_submit(e, sample, w, &ticket);
+        if (s != CE_OK) return s;
+        size_t n = 0;
+        return ce_poll(e, 600000000, &got, out.data(), out.size(), &n, busy);
+    };
+    double warm = 0.0;
+    ce_status s = time_one(&warm);
+    if (s != CE_OK) return s;
+    double best_s = 1e300;
+    unsigned best_cta = keep_cta, best_chunk = keep_chunk, best_small = keep_small;
+    for (unsigned cta : {0u, 3u}) {
+        for (unsigned chunk : {2u, 4u, 8u}) {
+            for (unsigned small : {12u, 16u, 24u}) {
+                e->ctas_per_sm = cta;
+                e->chunk_k = chunk;
+                e->small_body = small;
+                double busy = 0.0;
+                if ((s = time_one(&busy)) != CE_OK) {
+                    e->ctas_per_sm = keep_cta;
+                    e->chunk_k = keep_chunk;
+                    e->small_body = keep_small;
+                    return s;
+                }
+                if (busy < best_s) {
+                    best_s = busy;
+                    best_cta = cta;
+                    best_chunk = chunk;
+                    best_small = small;
+                }
+            }
+        }
+    }
+    e->ctas_per_sm = best_cta;
+    e->chunk_k = best_chunk;
+    e->small_body = best_small;
+    if (best) {
+        std::memset(best, 0, sizeof *best);
+        best->slots = (uint32_t)e->slots.size();
+        best->ctas_per_sm = best_cta;
+        best->chunk_k = best_chunk;
+        best->small_body = best_small;
+    }
+    if (seconds) *seconds = best_s;
     return CE_OK;
 }

@@ -3,12 +3,23 @@ of the engine against the reference kernel on the same case.
 
     python -m evolution_simulator_gpu_b200.profile_case --workload game \
         --creatures 300000 --seconds 1 [--reference]
+    python -m evolution_simulator_gpu_b200.profile_case --workload effects \
+        --creatures 3000000 --seconds 20 --generations 10 --autotune
 
 It generates the workload, runs one submission through the engine (one
 launch per size class) and prints the GPU seconds, the creature-substeps the
 trials ran and the bytes of the packed records. With --reference it also
 runs the reference's own kernel (oracle/_ref, built from its source) on the
 same batch and prints whether the results are equal to the bit.
+
+With --generations K it packs K generations of the workload (disjoint
+creature ranges), keeps them resident and runs them as one CUDA graph
+(GenerationGraph), once to warm up and once timed; with --autotune the
+engine's launch shape is first tuned on a sample of the workload.
+
+With --adjoint it runs the gradient path instead: one checkpointed forward
+run (ce_forward) and one backward run (ce_backward) of the workload, and
+prints both GPU times and the gradients per second.
 """
 from __future__ import annotations
 
@@ -29,7 +40,15 @@ def main() -> None:
     ap.add_argument("--seconds", type=float, default=1.0)
     ap.add_argument("--reference", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="resident blocks per SM (0: the engine's choice)")
+    ap.add_argument("--generations", type=int, default=0, help="run K resident generations as one CUDA graph")
+    ap.add_argument("--autotune", action="store_true", help="tune the launch shape on a sample first")
+    ap.add_argument("--sample", type=int, default=262_144, help="creatures in the autotune sample")
+    ap.add_argument("--adjoint", action="store_true", help="time forward + backward of the gradient path")
     args = ap.parse_args()
+    if args.generations:
+        return generations(args)
+    if args.adjoint:
+        return adjoint(args)
     import evolution_simulator_gpu_b200 as ce
     from evolution_simulator_gpu_b200.configs import WORKLOADS
     w = WORKLOADS[args.workload]
@@ -48,6 +67,50 @@ def main() -> None:
         ref, ms = RefKernel(ce.world_flags(world), world.rate or 60).run(wave, ce.make_params(world))
         out["reference_s"] = ms / 1e3
         out["bit_equal"] = bool((mine.view(np.uint32) == ref.view(np.uint32)).all())
+    print(json.dumps(out))
+
+
+def adjoint(args) -> None:
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS[args.workload]
+    world = w.world(duration=args.seconds)
+    wave = ce.pack(ce.generate(w.spec, args.creatures), world)
+    with ce.Engine(0) as eng, eng.forward(wave, world) as tape:
+        g = tape.backward()
+        fwd, bwd = tape.seconds
+        rows, mm = tape.shape
+    print(json.dumps({"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds,
+                      "rows": rows, "muscle_slots": mm, "forward_s": fwd, "backward_s": bwd,
+                      "finite": float(np.isfinite(g).all(axis=1).mean()),
+                      "gradients_per_s": args.creatures / (fwd + bwd)}))
+
+
+def generations(args) -> None:
+    import time
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS[args.workload]
+    world = w.world(duration=args.seconds)
+    out = {"workload": args.workload, "creatures": args.creatures, "seconds": args.seconds,
+           "generations": args.generations}
+    t0 = time.perf_counter()
+    waves = [ce.pack(ce.generate(w.spec, args.creatures, first=k * args.creatures), world)
+             for k in range(args.generations)]
+    out["pack_s"] = time.perf_counter() - t0
+    out["record_bytes"] = int(sum(v.lanes.nbytes + v.muscles.nbytes + v.heads.nbytes for v in waves))
+    with ce.Engine(0, ctas_per_sm=args.ctas_per_sm) as eng:
+        if args.autotune:
+            sample = ce.pack(ce.generate(w.spec, args.sample, first=args.generations * args.creatures), world)
+            out["launch_shape"], out["autotune_best_s"] = eng.autotune(sample, world)
+        with ce.GenerationGraph(eng, waves, world) as g:
+            out["warm_s"] = g.launch()
+            out["graph_s"] = g.launch()
+            subs = sum(ce.creature_substeps(g.results(k), world) for k in range(len(waves)))
+        # One generation as a plain submission, for the per-launch comparison.
+        _, out["plain_one_s"] = eng.run(waves[0], world)
+    out["creature_substeps"] = subs
+    out["creature_substeps_per_s"] = subs / out["graph_s"]
     print(json.dumps(out))
 
 

@@ -283,12 +283,21 @@ typedef struct ce_engine ce_engine;
 
 typedef struct ce_options {
     uint32_t slots;          /* concurrent submissions, 0 = default (4) */
-    uint32_t ctas_per_sm;    /* 0 = autotuned */
-    uint32_t warps_per_cta;  /* 0 = autotuned */
-    uint32_t reserved[5];
+    uint32_t ctas_per_sm;    /* resident blocks an SM, 0 = as many as fit */
+    uint32_t warps_per_cta;  /* reserved, 0 (blocks are 4 warps) */
+    uint32_t chunk_k;        /* claims shrink to 1/chunk_k of a queue's rest a warp, 0 = 4 */
+    uint32_t small_body;     /* most nodes of the first size class, 0 = 16 */
+    uint32_t reserved[3];
 } ce_options;
 
 ce_status ce_open(int device, const ce_options* options, ce_engine** out);
+/* Times `sample` (a packed batch like the ones to come) in `world` under a
+ * grid of launch settings (blocks an SM, claim chunk divisor, size-class
+ * split) and keeps the fastest for the engine's later submissions; `best`
+ * (optional) receives it and `seconds` (optional) its GPU time. No
+ * counterpart in the reference, whose launch shape is fixed. */
+ce_status ce_autotune(ce_engine* engine, const ce_wave_pack* sample, const ce_world* world, ce_options* best,
+                      double* seconds);
 ce_status ce_close(ce_engine* engine);
 const char* ce_last_error(void);
 
