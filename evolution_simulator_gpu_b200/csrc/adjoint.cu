@@ -1,5 +1,7 @@
 // Gradients of a creature's fitness by the adjoint method, in the calm world
-// (flat ground, gravity, air drag on the bones, no other effect).
+// (flat ground, gravity, air drag on the bones, no other effect) and in the
+// effects worlds (rough and sloped ground with hurdles, optionally shaken by
+// tremors, wind, thick air, water with buoyancy and drag, ice patches).
 //
 // Fitness is the centre of mass's x after the trial's last step (the fall
 // step for a creature that falls, shaders/creature.cu:1060-1064, 1193-1194).
@@ -28,6 +30,8 @@
 // friction, its mass and its start position. The host maps them to the genes.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "trial.cuh"
 
 namespace cek {
@@ -35,6 +39,34 @@ namespace cek {
 namespace {
 
 using CalmWorld = StaticWorld<kWorldCalm>;
+using EffectsWorld = StaticWorld<kWorldEffects>;
+using QuakeWorld = StaticWorld<kWorldEffectsQuake>;
+
+// d slope / d x of the ground under x: the terrain's second derivative (the
+// slope, gap and hurdle terms are linear in x between their kinks).
+template <class W>
+__device__ __forceinline__ float ground_curvature(const W& w, float x, float amp, float qphase) {
+    if (!w.has(CE_FLAG_TERRAIN)) {
+        return 0.0f;
+    }
+    const float u0 = fracf(x * (1.0f / 1.1f) + qphase);
+    const float u1 = fracf(x * (1.0f / 0.43f) + 0.3f + qphase);
+    const float c0 = (1.0f - 2.0f * u0) * (1.0f - 2.0f * u0) - 2.0f * u0 * (1.0f - u0);
+    const float c1 = (1.0f - 2.0f * u1) * (1.0f - 2.0f * u1) - 2.0f * u1 * (1.0f - u1);
+    return amp * (0.65f * 32.0f * c0 * (1.0f / (1.1f * 1.1f)) + 0.35f * 32.0f * c1 * (1.0f / (0.43f * 0.43f)));
+}
+
+// d ice_at / d x (the smoothstep of ice_at; 0 outside its ramps).
+__device__ __forceinline__ float ice_slope(float x) {
+    const float w = fracf(x * kIceInv);
+    const float t = fabsf(w - 0.5f) * 2.0f;
+    const float z = (0.7f - t) * 2.5f;
+    if (z < 0.0f || z > 1.0f) {
+        return 0.0f;
+    }
+    const float dt = (w - 0.5f < 0.0f ? -2.0f : 2.0f) * kIceInv;
+    return 6.0f * z * (1.0f - z) * -2.5f * dt;
+}
 
 // Lines of a lane's slot after the creature's constant lines (SlotLayout).
 struct AdjointLayout {
@@ -97,11 +129,11 @@ struct AdjointArgs {
     const float* weights;   // dL/dfitness a creature (packed index), NULL for 1
 };
 
-template <int RATE>
+template <class W, int RATE>
 struct Backward {
     using C = Clock<RATE>;
-    using Body = Creature<CalmWorld, RATE, false>;
-    using T = Trial<CalmWorld, false, RATE>;
+    using Body = Creature<W, RATE, false>;
+    using T = Trial<W, false, RATE>;
     const Body& b;
     const NodeTables& g;  // adjoints: positions, velocities, start positions / forces, (energy, demand)
     const AdjointLayout& A;
@@ -237,8 +269,24 @@ struct Backward {
             L.put(A.drag + j, make_float4(v0.x, v0.y, v1.x, v1.y));
             const float wx = 0.5f * (v0.x + v1.x), wy = 0.5f * (v0.y + v1.y);
             const float speed = sqrtf(wx * wx + wy * wy);
-            const float k_air = fminf(bb.x * speed, bb.y);
-            const float dfx = -wx * k_air, dfy = -wy * k_air;
+            const float limit = bb.y;
+            const float k_air = fminf(bb.x * speed, limit);
+            float dfx = -wx * k_air, dfy = -wy * k_air;
+            if (b.w.has(CE_FLAG_WATER)) {
+                const float r0 = L.get(S.node + i0).z, r1 = L.get(S.node + i1).z;
+                const float width = r0 + r1;
+                const float2 p0 = t.pos(i0), p1 = t.pos(i1);
+                const float wet0 = clampf((b.p.water - (p0.y - r0)) / (2.0f * r0), 0.0f, 1.0f);
+                const float wet1 = clampf((b.p.water - (p1.y - r1)) / (2.0f * r1), 0.0f, 1.0f);
+                const float wet = 0.5f * (wet0 + wet1);
+                const float ax = (p1.x - p0.x) / ba.y, ay = (p1.y - p0.y) / ba.y;
+                const float along = wx * ax + wy * ay;
+                const float lx = ax * along, ly = ay * along;
+                const float sx = wx - lx, sy = wy - ly;
+                const float k_water = fminf(kWaterDrag * wet * ba.y * width * speed, limit);
+                dfx -= sx * k_water + lx * k_water * kWaterAlong;
+                dfy -= sy * k_water + ly * k_water * kWaterAlong;
+            }
             t.vel(i0) = make_float2(v0.x + bb.z * dfx, v0.y + bb.z * dfy);
             t.vel(i1) = make_float2(v1.x + bb.w * dfx, v1.y + bb.w * dfy);
         }
@@ -250,6 +298,10 @@ struct Backward {
             reinterpret_cast<float2*>(&L.base[(A.force + i / 2u) * 32u])[i % 2u] = fpv;
             s.z += C::h * (f.x + fpv.x) * nr.y;
             s.w += C::h * (f.y + fpv.y) * nr.y;
+            if (b.w.has(CE_FLAG_AIR)) {
+                s.z *= b.p.air_sub;
+                s.w *= b.p.air_sub;
+            }
             t.f(i) = make_float2(s.x, s.y);
             s.x += C::h * s.z;
             s.y += C::h * s.w;
@@ -307,13 +359,11 @@ struct Backward {
             const float2 before = q;
             b.solve_ground(i, nr, q, f0);
             // The ground pass's contact and stick/slip tests, on the same
-            // values (flat ground: unit normal, slide along x).
-            const float depth = ground_depth(before.y, nr);
-            if (depth > 0.0f) {
+            // values.
+            const Contact c = contact(before, f0, nr);
+            if (c.depth > 0.0f) {
                 touch |= 1u << i;
-                const float slide = before.x - f0.x;
-                const float budget = nr.w * b.p.friction * depth;
-                if (!(fabsf(slide) <= budget)) {
+                if (!(fabsf(c.slide) <= c.mu * c.depth)) {
                     slip |= 1u << i;
                 }
             }
@@ -339,12 +389,87 @@ struct Backward {
         return violated;
     }
 
-    // Depth of a node below the flat ground (the ground pass's arithmetic:
-    // slope 0, so the secant is 1).
-    __device__ __forceinline__ static float ground_depth(float y, const float4& nr) {
-        const float secant = sqrtf(1.0f + 0.0f * 0.0f);
-        const float dry = (y - 0.0f) / secant - nr.z;
-        return -dry;
+    // The ground pass's contact of a node at q (Creature::solve_ground's
+    // arithmetic): the ground's height and slope under q.x, its secant and
+    // normal, the depth, the friction coefficient and the slide along the
+    // surface after the push out.
+    struct Contact {
+        float2 gr, n, q1;
+        float secant, depth, mu, ice, slide;
+    };
+    __device__ __forceinline__ Contact contact(float2 q, float2 f0, const float4& nr) const {
+        Contact c;
+        c.gr = ground(b.w, q.x, b.r.amp, b.r.qphase, b.p);
+        c.secant = sqrtf(1.0f + c.gr.y * c.gr.y);
+        c.n = make_float2(-c.gr.y / c.secant, 1.0f / c.secant);
+        const float dry = (q.y - c.gr.x) / c.secant - nr.z;
+        c.depth = -dry;
+        c.mu = nr.w * b.p.friction;
+        c.ice = 1.0f;
+        if (b.w.has(CE_FLAG_ICE)) {
+            c.ice = 1.0f - b.p.patches * ice_at(q.x);
+            c.mu *= c.ice;
+        }
+        c.q1 = make_float2(q.x + c.n.x * c.depth, q.y + c.n.y * c.depth);
+        const float tx = c.n.y, ty = -c.n.x;
+        c.slide = (c.q1.x - f0.x) * tx + (c.q1.y - f0.y) * ty;
+        return c;
+    }
+
+    // Adjoint of node i's ground contact (pushed out along the normal, then
+    // held or slid back along the surface) from the position before it `q`,
+    // the substep's start position `f0` and the adjoint of the result in the
+    // table; the start position's share goes to g.f.
+    __device__ __forceinline__ void ground_back(unsigned i, const float4& nr, float2 q, float2 f0,
+                                                bool slipped) const {
+        const Contact c = contact(q, f0, nr);
+        const float S = c.gr.y, sec = c.secant, nx = c.n.x, ny = c.n.y;
+        const float tx = ny, ty = -nx;
+        const float budget = c.mu * c.depth;
+        const float back = slipped ? copysignf(budget, c.slide) : c.slide;
+        const float2 l2 = g.pos(i);
+        float2 lq1 = l2;
+        float ltx = -back * l2.x, lty = -back * l2.y;
+        const float lback = -(l2.x * tx + l2.y * ty);
+        float ldepth = 0.0f, lmu = 0.0f, lslide = 0.0f;
+        if (slipped) {
+            const float lbudget = c.slide < 0.0f ? -lback : lback;
+            lmu = lbudget * c.depth;
+            ldepth = lbudget * c.mu;
+        } else {
+            lslide = lback;
+        }
+        lq1.x += lslide * tx;
+        lq1.y += lslide * ty;
+        float2 lf = g.f(i);
+        lf.x -= lslide * tx;
+        lf.y -= lslide * ty;
+        g.f(i) = lf;
+        ltx += lslide * (c.q1.x - f0.x);
+        lty += lslide * (c.q1.y - f0.y);
+        float lny = ltx, lnx = -lty;
+        float2 lq = lq1;
+        lnx += lq1.x * c.depth;
+        lny += lq1.y * c.depth;
+        ldepth += lq1.x * nx + lq1.y * ny;
+        float lx = 0.0f;
+        if (lmu != 0.0f) {
+            b.L.word(A.fric + i / 4u, i % 4u) += lmu * b.p.friction * c.ice;
+            if (b.w.has(CE_FLAG_ICE)) {
+                lx -= lmu * nr.w * b.p.friction * b.p.patches * ice_slope(q.x);
+            }
+        }
+        // depth = radius - (q.y - height) / secant
+        lq.y -= ldepth / sec;
+        const float lheight = ldepth / sec;
+        float lsec = ldepth * (q.y - c.gr.x) / (sec * sec);
+        // n = (-slope, 1) / secant, secant = sqrt(1 + slope^2)
+        float lslope = -lnx / sec;
+        lsec += (lnx * S - lny) / (sec * sec);
+        lslope += lsec * S / sec;
+        lx += lheight * S + lslope * ground_curvature(b.w, q.x, b.r.amp, b.r.qphase);
+        lq.x += lx;
+        g.pos(i) = lq;
     }
 
     // A push node += w lam g with lam = -e / wgt, wgt = sum w |g|^2: the
@@ -430,33 +555,14 @@ struct Backward {
             g.f(i) = make_float2(-lv.x * C::inv_h, -lv.y * C::inv_h);
             g.vel(i) = make_float2(0.0f, 0.0f);
         }
-        // Ground contact on flat ground: the height goes to the surface; a
-        // sticking node goes back to its start x, a sliding one moves by
-        // friction x depth.
+        // Ground contact.
         for (unsigned i = 0u; i < r.nodes; i++) {
             if (((touch >> i) & 1u) == 0u) {
                 continue;
             }
             const float4 nr = L.get(S.node + i);
             const float* pj = reinterpret_cast<const float*>(&L.base[(A.pj + i / 2u) * 32u]) + 2u * (i % 2u);
-            const float2 q = make_float2(pj[0], pj[1]);
-            const float2 f0 = t.f(i);
-            const float2 lq = g.pos(i);
-            if ((slip >> i) & 1u) {
-                const float depth = ground_depth(q.y, nr);
-                const float slide = q.x - f0.x;
-                const float sigma = slide < 0.0f ? -1.0f : 1.0f;
-                const float mu = nr.w * p.friction;
-                g.pos(i) = make_float2(lq.x, lq.x * sigma * mu);
-                const float gmu = -lq.x * sigma * depth * p.friction;
-                float* fr = &L.word(A.fric + i / 4u, i % 4u);
-                *fr += gmu;
-            } else {
-                g.pos(i) = make_float2(0.0f, 0.0f);
-                float2 lf = g.f(i);
-                lf.x += lq.x;
-                g.f(i) = lf;
-            }
+            ground_back(i, nr, make_float2(pj[0], pj[1]), t.f(i), ((slip >> i) & 1u) != 0u);
         }
         // Joint limits, last to first, on the joints that were pushed.
         for (unsigned j = bones; j-- > 1u;) {
@@ -492,15 +598,29 @@ struct Backward {
             add_inverse_mass(i0, w0, sc * (dx * l0.x + dy * l0.y) + lsw);
             add_inverse_mass(i1, w1, -sc * (dx * l1.x + dy * l1.y) + lsw);
         }
-        // Integration: q1 = q0 + h v1, v1 = v + h (f_world + f_muscle) / m,
-        // and the start position kept for the velocity pass.
-        // Mass: v1 = v + h (-g m + F) / m, whose m-derivative is -h F / m^2
-        // (gravity's share cancels).
+        // Integration: q1 = q0 + h v1, v1 = a (v + h (f_world + f_muscle) / m)
+        // (a the thick air's retention, 1 without), and the start position
+        // kept for the velocity pass. Mass: the world force is a mass times
+        // an acceleration (gravity, wind, buoyancy), so the m-derivative of
+        // v1 is -a h F / m^2. Buoyancy's depth goes to the start height.
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float im = L.get(S.node + i).y;
+            const float4 nr = L.get(S.node + i);
+            const float im = nr.y;
             const float2 lq1 = g.pos(i), lq0 = g.f(i);
-            g.pos(i) = make_float2(lq1.x + lq0.x, lq1.y + lq0.y);
-            const float2 lv1 = make_float2(C::h * lq1.x, C::h * lq1.y);
+            float2 lp = make_float2(lq1.x + lq0.x, lq1.y + lq0.y);
+            float2 lv1 = make_float2(C::h * lq1.x, C::h * lq1.y);
+            if (b.w.has(CE_FLAG_AIR)) {
+                lv1.x *= p.air_sub;
+                lv1.y *= p.air_sub;
+            }
+            if (b.w.has(CE_FLAG_WATER)) {
+                const float y0 = tape.pair(k_tape, 2u * i)->y;
+                const float z = (p.water - (y0 - nr.z)) / (2.0f * nr.z);
+                if (z >= 0.0f && z <= 1.0f) {
+                    lp.y -= lv1.y * C::h * im * kWaterBuoyancy * nr.x * p.gravity / (2.0f * nr.z);
+                }
+            }
+            g.pos(i) = lp;
             g.vel(i) = lv1;
             g.f(i) = make_float2(lv1.x * C::h * im, lv1.y * C::h * im);
             const float2 F = reinterpret_cast<const float2*>(&L.base[(A.force + i / 2u) * 32u])[i % 2u];
@@ -513,24 +633,78 @@ struct Backward {
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float wx = 0.5f * (pre.x + pre.z), wy = 0.5f * (pre.y + pre.w);
             const float speed = sqrtf(wx * wx + wy * wy);
-            const float k_air = fminf(bb.x * speed, bb.y);
+            const float limit = bb.y;
+            const float k_air = fminf(bb.x * speed, limit);
             const float2 l0 = g.vel(i0), l1 = g.vel(i1);
             const float ldx = bb.z * l0.x + bb.w * l1.x, ldy = bb.z * l0.y + bb.w * l1.y;
             float lwx = -k_air * ldx, lwy = -k_air * ldy;
             const float lk = -(wx * ldx + wy * ldy);
-            if (bb.x * speed <= bb.y) {
-                if (speed > 0.0f) {
-                    const float lsp = lk * bb.x;
-                    lwx += lsp * wx / speed;
-                    lwy += lsp * wy / speed;
-                }
+            float lspeed = 0.0f, llimit = 0.0f;
+            if (bb.x * speed <= limit) {
+                lspeed += lk * bb.x;
             } else {
+                llimit += lk;
+            }
+            float dfx = -wx * k_air, dfy = -wy * k_air;
+            if (b.w.has(CE_FLAG_WATER)) {
+                // Water drag from the bone's wet share at the substep's start
+                // positions: across the bone in full, along it by kWaterAlong.
+                const float r0 = L.get(S.node + i0).z, r1 = L.get(S.node + i1).z;
+                const float width = r0 + r1;
+                const float2 p0 = *tape.pair(k_tape, 2u * i0), p1 = *tape.pair(k_tape, 2u * i1);
+                const float z0 = (p.water - (p0.y - r0)) / (2.0f * r0);
+                const float z1 = (p.water - (p1.y - r1)) / (2.0f * r1);
+                const float wet = 0.5f * (clampf(z0, 0.0f, 1.0f) + clampf(z1, 0.0f, 1.0f));
+                const float ax = (p1.x - p0.x) / ba.y, ay = (p1.y - p0.y) / ba.y;
+                const float along = wx * ax + wy * ay;
+                const float lx = ax * along, ly = ay * along;
+                const float sx = wx - lx, sy = wy - ly;
+                const float xw = kWaterDrag * wet * ba.y * width * speed;
+                const float k_water = fminf(xw, limit);
+                dfx -= sx * k_water + lx * k_water * kWaterAlong;
+                dfy -= sy * k_water + ly * k_water * kWaterAlong;
+                const float lkw = -(sx * ldx + sy * ldy) - kWaterAlong * (lx * ldx + ly * ldy);
+                // s = w - l, l = a (w . a)
+                const float lsx = -k_water * ldx, lsy = -k_water * ldy;
+                const float llx = -k_water * kWaterAlong * ldx - lsx, lly = -k_water * kWaterAlong * ldy - lsy;
+                lwx += lsx;
+                lwy += lsy;
+                const float lalong = llx * ax + lly * ay;
+                lwx += lalong * ax;
+                lwy += lalong * ay;
+                const float lax = llx * along + lalong * wx, lay = lly * along + lalong * wy;
+                float lwet = 0.0f;
+                if (xw <= limit) {
+                    lwet = lkw * kWaterDrag * ba.y * width * speed;
+                    lspeed += lkw * kWaterDrag * wet * ba.y * width;
+                } else {
+                    llimit += lkw;
+                }
+                float2 e = g.pos(i0);
+                e.x -= lax / ba.y;
+                e.y -= lay / ba.y;
+                if (z0 >= 0.0f && z0 <= 1.0f) {
+                    e.y -= 0.5f * lwet / (2.0f * r0);
+                }
+                g.pos(i0) = e;
+                e = g.pos(i1);
+                e.x += lax / ba.y;
+                e.y += lay / ba.y;
+                if (z1 >= 0.0f && z1 <= 1.0f) {
+                    e.y -= 0.5f * lwet / (2.0f * r1);
+                }
+                g.pos(i1) = e;
+            }
+            if (speed > 0.0f) {
+                lwx += lspeed * wx / speed;
+                lwy += lspeed * wy / speed;
+            }
+            if (llimit != 0.0f) {
                 // The limit 0.5 (m0 + m1) / h.
-                add_mass(i0, 0.5f * C::inv_h * lk);
-                add_mass(i1, 0.5f * C::inv_h * lk);
+                add_mass(i0, 0.5f * C::inv_h * llimit);
+                add_mass(i1, 0.5f * C::inv_h * llimit);
             }
             // The scales 0.5 h / m of the two ends.
-            const float dfx = -wx * k_air, dfy = -wy * k_air;
             add_inverse_mass(i0, L.get(S.node + i0).y, 0.5f * C::h * (l0.x * dfx + l0.y * dfy));
             add_inverse_mass(i1, L.get(S.node + i1).y, 0.5f * C::h * (l1.x * dfx + l1.y * dfy));
             g.vel(i0) = make_float2(l0.x + 0.5f * lwx, l0.y + 0.5f * lwy);
@@ -863,11 +1037,11 @@ struct Backward {
     }
 };
 
-template <int RATE>
+template <class W, int RATE>
 __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, const ce_params p,
                                                             const AdjointArgs x) {
     extern __shared__ float4 smem[];
-    using B = Backward<RATE>;
+    using B = Backward<W, RATE>;
     const unsigned threads = blockDim.x;
     float2* const tables = reinterpret_cast<float2*>(smem) + threadIdx.x;
     const size_t node_table = (size_t)a.rows * threads, muscle_table = (size_t)(a.mm > 0u ? a.mm : 1u) * threads;
@@ -882,7 +1056,7 @@ __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, 
     const Lines L{a.scratch + (size_t)warp * A.lines * 32u + lane};
     const unsigned tl = tape_lines(a.rows, a.mm);
     const Tape tape{x.tape + (size_t)warp * 256u * tl * 32u + lane, tl};
-    const CalmWorld w{};
+    const W w{};
     LaneRegs r;
     const typename B::Body body{w, p, tab, L, S, r};
     unsigned end = 0u, seg = 0u;
@@ -931,46 +1105,60 @@ size_t adjoint_tape_bytes(unsigned grid, unsigned rows, unsigned mm) {
     return warps * 256u * (size_t)tape_lines(rows, mm) * 32u * 16u;
 }
 
-cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, int rate, int* blocks) {
+// The worlds with gradients, as compile-time worlds: f(world, rate).
+template <class F>
+cudaError_t with_gradient_world(uint32_t flags, int rate, F&& f) {
+    auto at = [&](auto w) -> cudaError_t {
+        if (rate == 60) return f(w, std::integral_constant<int, 60>{});
+        if (rate == 120) return f(w, std::integral_constant<int, 120>{});
+        return cudaErrorInvalidValue;
+    };
+    switch (flags) {
+        case kWorldCalm: return at(CalmWorld{});
+        case kWorldEffects: return at(EffectsWorld{});
+        case kWorldEffectsQuake: return at(QuakeWorld{});
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+bool gradient_world(uint32_t flags) {
+    return flags == kWorldCalm || flags == kWorldEffects || flags == kWorldEffectsQuake;
+}
+
+cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, uint32_t flags, int rate, int* blocks) {
     const size_t smem = adjoint_smem_bytes(rows, mm, kBlock);
-    auto go = [&](auto kern) -> cudaError_t {
+    return with_gradient_world(flags, rate, [&](auto w, auto r) -> cudaError_t {
+        auto kern = adjoint_kernel<decltype(w), decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kern, (int)kBlock, smem);
-    };
-    if (rate == 60) return go(adjoint_kernel<60>);
-    if (rate == 120) return go(adjoint_kernel<120>);
-    return cudaErrorInvalidValue;
+    });
 }
 
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p) {
-    if (s.flags != kWorldCalm || s.record || a.rows != s.rows || a.mm != s.mm) return cudaErrorInvalidValue;
+    if (s.record || a.rows != s.rows || a.mm != s.mm) return cudaErrorInvalidValue;
     const size_t smem = smem_bytes(s.rows, s.mm, s.block);
-    auto go = [&](auto kern) -> cudaError_t {
+    return with_gradient_world(s.flags, s.rate, [&](auto w, auto r) -> cudaError_t {
+        auto kern = advance_kernel<decltype(w), false, decltype(r)::value, true>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, CalmWorld{});
+        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, w);
         return cudaGetLastError();
-    };
-    if (s.rate == 60) return go(advance_kernel<CalmWorld, false, 60, true>);
-    if (s.rate == 120) return go(advance_kernel<CalmWorld, false, 120, true>);
-    return cudaErrorInvalidValue;
+    });
 }
 
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
                            const float* weights) {
-    if (s.flags != kWorldCalm || s.record || a.rows != s.rows || a.mm != s.mm) return cudaErrorInvalidValue;
+    if (s.record || a.rows != s.rows || a.mm != s.mm) return cudaErrorInvalidValue;
     const size_t smem = adjoint_smem_bytes(s.rows, s.mm, s.block);
     const AdjointArgs x{tape, grads, weights};
-    auto go = [&](auto kern) -> cudaError_t {
+    return with_gradient_world(s.flags, s.rate, [&](auto w, auto r) -> cudaError_t {
+        auto kern = adjoint_kernel<decltype(w), decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         kern<<<s.grid, s.block, smem, s.stream>>>(a, p, x);
         return cudaGetLastError();
-    };
-    if (s.rate == 60) return go(adjoint_kernel<60>);
-    if (s.rate == 120) return go(adjoint_kernel<120>);
-    return cudaErrorInvalidValue;
+    });
 }
 
 }  // namespace cek

@@ -619,6 +619,7 @@ struct ce_tape {
     cudaEvent_t start = nullptr, stop = nullptr;
     size_t count = 0;
     unsigned rows = 2, mm = 0, ckpts = 0, grid = 1;
+    uint32_t flags = 0;
     int rate = 60;
     ce_params params{};
     DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_buckets, d_ckpt, d_ends, d_scratch, d_tape, d_grads,
@@ -669,8 +670,10 @@ extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce
     *out = nullptr;
     ce_status s = check_world(w);
     if (s != CE_OK) return s;
-    if (ce_world_flags(w) != cek::kWorldCalm) {
-        set_error("ce_forward: gradients are built for the calm world (flat ground, no effects)");
+    const uint32_t flags = ce_world_flags(w);
+    if (!cek::gradient_world(flags)) {
+        set_error("ce_forward: gradients are built for the calm world and the effects worlds (without mud, "
+                  "brambles or gaps)");
         return CE_ERR_UNSUPPORTED;
     }
     if (checkpoint_every != 256u) {
@@ -690,6 +693,7 @@ extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce
     ce_tape* t = new ce_tape;
     t->engine = e;
     t->count = pack->count;
+    t->flags = flags;
     for (const ClassPlan& c : plans) {
         t->rows = std::max(t->rows, c.rows);
         t->mm = std::max(t->mm, c.mm);
@@ -710,7 +714,7 @@ extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce
     const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
     const size_t res_b = pack->count * sizeof(ce_result);
     const size_t ckpt_b = pack->count * (size_t)t->ckpts * cek::checkpoint_floats(t->rows, t->mm) * 4;
-    t->grid = grid_for(e, t->rows, t->mm, cek::kWorldCalm, false, t->rate, pack->count);
+    t->grid = grid_for(e, t->rows, t->mm, flags, false, t->rate, pack->count);
     if ((s = t->d_lanes.ensure(lanes_b)) || (s = t->d_muscles.ensure(std::max<size_t>(mus_b, 4))) ||
         (s = t->d_heads.ensure(heads_b)) || (s = t->d_results.ensure(res_b)) ||
         (s = t->d_buckets.ensure(cek::bucket_bytes(pack->count))) || (s = t->d_ckpt.ensure(ckpt_b)) ||
@@ -737,7 +741,7 @@ extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce
     }
     cek::KernelArgs a = tape_args(t, bk);
     a.scratch = static_cast<float4*>(t->d_scratch.ptr);
-    cek::LaunchSpec ls{t->rows, t->mm, cek::kWorldCalm, false, t->rate, t->grid, cek::kBlock, st};
+    cek::LaunchSpec ls{t->rows, t->mm, flags, false, t->rate, t->grid, cek::kBlock, st};
     if ((s = cuda_status(cek::launch_forward_ckpt(ls, a, t->params), "forward launch")) ||
         (s = cuda_status(cudaEventRecord(t->stop, st), "cudaEventRecord")) ||
         (s = tape_time(t, &t->forward_seconds))) {
@@ -783,7 +787,7 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
     ce_status s = set_device(t->engine);
     if (s != CE_OK) return s;
     int per_sm = 0;
-    if (cek::adjoint_occupancy(t->rows, t->mm, t->rate, &per_sm) != cudaSuccess || per_sm < 1) {
+    if (cek::adjoint_occupancy(t->rows, t->mm, t->flags, t->rate, &per_sm) != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;
     }
@@ -807,7 +811,7 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
            "bucketing launch");
     cek::KernelArgs a = tape_args(t, bk);
     a.scratch = static_cast<float4*>(t->d_scratch.ptr);
-    cek::LaunchSpec ls{t->rows, t->mm, cek::kWorldCalm, false, t->rate, grid, cek::kBlock, st};
+    cek::LaunchSpec ls{t->rows, t->mm, t->flags, false, t->rate, grid, cek::kBlock, st};
     CE_TRY(cek::launch_adjoint(ls, a, t->params, static_cast<float4*>(t->d_tape.ptr),
                                static_cast<float*>(t->d_grads.ptr),
                                dl_dfitness ? static_cast<const float*>(t->d_weights.ptr) : nullptr),

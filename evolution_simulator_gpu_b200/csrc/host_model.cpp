@@ -963,11 +963,30 @@ extern "C" ce_status ce_gene_gradients(const ce_population* pop, const uint32_t*
         std::vector<double> dmass(n, 0.0);
         for (size_t node = 0; node < n; node++) dmass[node] = rec[9 * mm + rows + row_of[node]];
         // The start pose is moved by minus the centre of mass's x
-        // (start_state), so a mass moves every start x by -x_start / total.
+        // (start_state), so a mass moves every start x by -x_start / total;
+        // on uneven ground it is also lowered onto the ground under its
+        // lowest node, whose height moves with the shift by the ground's
+        // slope there.
         {
             const State st = start_state(M, *world);
-            double shift = 0.0;
-            for (size_t r = 0; r < n; r++) shift += rec[9 * mm + 2 * rows + 2 * r];
+            double shift = 0.0, lift = 0.0;
+            for (size_t r = 0; r < n; r++) {
+                shift += rec[9 * mm + 2 * rows + 2 * r];
+                lift += rec[9 * mm + 2 * rows + 2 * r + 1];
+            }
+            if (world->ground) {
+                float lowest = std::numeric_limits<float>::infinity(), slope = 0.0f;
+                for (size_t r = 0; r < n; r++) {
+                    float h, sl;
+                    ground(st.px[r], M.amplitude, world->slope, world->gaps, world->hurdles, M.quake_phase_, h, sl);
+                    const float low = st.py[r] - M.radius[r] - fmax_(h, -1e6f);
+                    if (low < lowest) {
+                        lowest = low;
+                        slope = sl;
+                    }
+                }
+                shift += lift * (double)slope;
+            }
             for (size_t node = 0; node < n; node++) {
                 dmass[node] -= shift * (double)st.px[row_of[node]] * (double)M.inv_mass;
             }

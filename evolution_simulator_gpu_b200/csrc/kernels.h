@@ -80,7 +80,9 @@ __host__ __device__ inline unsigned grad_floats(unsigned rows, unsigned mm) { re
 size_t adjoint_smem_bytes(unsigned rows, unsigned mm, unsigned block);
 size_t adjoint_slot_bytes(unsigned grid, unsigned rows, unsigned mm);   // lane slots of the backward grid
 size_t adjoint_tape_bytes(unsigned grid, unsigned rows, unsigned mm);   // segment tapes of the backward grid
-cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, int rate, int* blocks);
+// Worlds the gradient kernels are built for: calm, effects, effects + tremors.
+bool gradient_world(uint32_t flags);
+cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, uint32_t flags, int rate, int* blocks);
 struct LaunchSpec;
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,

@@ -355,8 +355,11 @@ ce_status ce_graph_close(ce_graph* graph);
 
 /* Gradients of fitness (no counterpart in the reference, which has no
  * derivatives): a forward/backward pair shaped like an autograd function.
- * ce_forward runs the batch in the calm world (flat ground, no effects;
- * CE_ERR_UNSUPPORTED otherwise, or for muscles with touch sensors) with a
+ * ce_forward runs the batch in the calm world (flat ground, no effects) or
+ * in an effects world (rough, sloped ground with hurdles, tremors, water,
+ * ice, wind, thick air: the flag sets of the effects workloads;
+ * CE_ERR_UNSUPPORTED for other flag sets, with mud, brambles or gaps, or for
+ * muscles with touch sensors) with a
  * checkpoint of each creature's state every `checkpoint_every` substeps
  * (256 only) and keeps what the backward pass needs in the tape; its results
  * equal ce_submit's to the bit. ce_backward returns, for every creature in

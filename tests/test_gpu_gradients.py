@@ -21,6 +21,7 @@ from oracle.ref import Oracle
 pytestmark = pytest.mark.gpu
 
 W = WORKLOADS["gradients"]
+R = WORKLOADS["refine"]
 
 
 def _record_direction(wave, rows, mm, rng):
@@ -41,21 +42,27 @@ def _project(g, rows, mm, dm, dn, dmass):
             + (g[:, 9 * mm + rows:9 * mm + 2 * rows] * dmass).sum(axis=1))
 
 
-def test_forward_results_equal_the_plain_kernel(engine):
-    world = W.world(duration=2.0)
-    wave = ce.pack(ce.generate(W.spec, 4096), world)
+@pytest.mark.parametrize("name,quake", [("gradients", True), ("refine", True), ("refine", False)])
+def test_forward_results_equal_the_plain_kernel(engine, name, quake):
+    w = WORKLOADS[name]
+    world = w.world(duration=2.0) if quake else w.world(duration=2.0, quake=0.0)
+    wave = ce.pack(ce.generate(w.spec, 4096), world)
     plain, _ = engine.run(wave, world)
     with engine.forward(wave, world) as tape:
         res = tape.results
     assert (res.view(np.uint32) == plain.view(np.uint32)).all()
 
 
-@pytest.mark.parametrize("seconds,median,share", [(0.05, 1e-4, 0.95), (0.25, 1e-3, 0.55)])
-def test_adjoint_matches_fp64_tangent(engine, seconds, median, share):
+@pytest.mark.parametrize("name,seconds,median,share", [("gradients", 0.05, 1e-4, 0.95), ("gradients", 0.25, 1e-3, 0.55),
+                                                       ("refine", 0.05, 1e-4, 0.9), ("refine", 0.25, 1e-3, 0.5)])
+def test_adjoint_matches_fp64_tangent(engine, name, seconds, median, share):
     """<gradient, u> against the FP64 tangent along u for 256 creatures, u a
-    random direction in all record fields (muscles, friction, mass)."""
-    world = W.world(duration=seconds)
-    wave = ce.pack(ce.generate(W.spec, 256), world)
+    random direction in all record fields (muscles, friction, mass), in the
+    calm world and in the refined-search world (rough ground with hurdles and
+    tremors, water, ice, wind, thick air)."""
+    w = WORKLOADS[name]
+    world = w.world(duration=seconds)
+    wave = ce.pack(ce.generate(w.spec, 256), world)
     with engine.forward(wave, world) as tape:
         g = tape.backward()
         rows, mm = tape.shape
@@ -69,12 +76,14 @@ def test_adjoint_matches_fp64_tangent(engine, seconds, median, share):
     assert (rel < 1e-3).mean() >= share, (rel < 1e-3).mean()
 
 
-def test_gene_gradients_match_fp64_differences(engine):
+@pytest.mark.parametrize("name", ["gradients", "refine"])
+def test_gene_gradients_match_fp64_differences(engine, name):
     """End to end: GPU record gradient, gene chain rule, against central
     differences of the FP64 host physics over repacked genes (h = 2e-4,
     mode-preserving perturbations: the one-sided differences agree)."""
-    world = W.world(duration=0.1)
-    pop = ce.generate(W.spec, 64)
+    w = WORKLOADS[name]
+    world = w.world(duration=0.1)
+    pop = ce.generate(w.spec, 64)
     wave = ce.pack(pop, world)
     with engine.forward(wave, world) as tape:
         g = tape.backward()
@@ -143,10 +152,10 @@ def test_backward_is_linear_in_the_fitness_weights(engine):
 
 
 def test_gradients_refuse_unsupported_batches(engine):
-    effects = ce.make_world(duration=1.0, **effects_world_kw())
-    wave = ce.pack(ce.generate(W.spec, 16), effects)
+    muddy = ce.make_world(duration=1.0, **dict(effects_world_kw(), mud=0.5))
+    wave = ce.pack(ce.generate(W.spec, 16), muddy)
     with pytest.raises(ce.EngineError) as err:
-        engine.forward(wave, effects)
+        engine.forward(wave, muddy)
     assert err.value.status == ce.CE_ERR_UNSUPPORTED
     world = W.world(duration=1.0)
     wave = ce.pack(ce.generate(W.spec, 16), world)

@@ -48,8 +48,14 @@ def _moved(pop, vm, vn, h):
     return ce.Population(n, pop.bones, m, pop.genomes, strength)
 
 
-def test_gene_chain_rule_matches_packer_differences():
-    w = WORKLOADS["gradients"]
+@pytest.mark.parametrize("workload,part", [("gradients", "all"), ("refine", "all"), ("gradients", "start"),
+                                           ("refine", "start")])
+def test_gene_chain_rule_matches_packer_differences(workload, part):
+    """In the calm world and in the refined-search world (rough ground with
+    hurdles, tremors and the other effects), where the start pose is also
+    lowered onto the ground under its lowest node; `start` puts the record
+    gradient on the start positions alone (the pose's shifts)."""
+    w = WORKLOADS[workload]
     world = w.world(duration=1.0)
     pop = ce.generate(w.spec, 48)
     assert pop.strength is not None
@@ -57,45 +63,69 @@ def test_gene_chain_rule_matches_packer_differences():
     rows, mm = int((wave.heads[:, 0] & 255).max()), int(wave.heads[:, 1].max())
     rng = np.random.default_rng(0)
     g = rng.normal(size=(len(wave), 9 * mm + 4 * rows)).astype(np.float32)
+    if part == "start":
+        g[:, :9 * mm + 2 * rows] = 0.0
     mg, ng = ce.gene_gradients(pop, wave, world, g, (rows, mm))
     vm, vn = _direction(pop, rng)
     h = 1e-3
     wp, wm = ce.pack(_moved(pop, vm, vn, h), world), ce.pack(_moved(pop, vm, vn, -h), world)
     assert (wp.slots == wave.slots).all() and (wm.slots == wave.slots).all()
-    lhs = 0.0
-    lfp, lfm = wp.lanes.view(np.float32), wm.lanes.view(np.float32)
-    for c in range(len(wave)):
+
+    def record_change(wa, wb, c):
+        """<g_c, records(wa) - records(wb)> of creature c."""
+        la, lb = wa.lanes.view(np.float32), wb.lanes.view(np.float32)
         M, N = int(wave.heads[c, 1]), int(wave.heads[c, 0] & 255)
         mo, ro = int(wave.heads[c, 4]), int(wave.heads[c, 3])
+        out = 0.0
         for k in range(M):
             for f, fi in enumerate(FIELDS):
-                d = (float(wp.muscles[mo + 20 * k + fi]) - float(wm.muscles[mo + 20 * k + fi])) / (2 * h)
-                lhs += float(g[c, 9 * k + f]) * d
+                out += float(g[c, 9 * k + f]) * (float(wa.muscles[mo + 20 * k + fi]) -
+                                                 float(wb.muscles[mo + 20 * k + fi]))
         for i in range(N):
-            d = (float(lfp[ro + 6 * i + 2]) - float(lfm[ro + 6 * i + 2])) / (2 * h)
-            lhs += float(g[c, 9 * mm + i]) * d
-            d = (float(lfp[ro + 6 * i]) - float(lfm[ro + 6 * i])) / (2 * h)
-            lhs += float(g[c, 9 * mm + rows + i]) * d
+            out += float(g[c, 9 * mm + i]) * (float(la[ro + 6 * i + 2]) - float(lb[ro + 6 * i + 2]))
+            out += float(g[c, 9 * mm + rows + i]) * (float(la[ro + 6 * i]) - float(lb[ro + 6 * i]))
             for axis in range(2):
-                d = (float(lfp[ro + 6 * i + 3 + axis]) - float(lfm[ro + 6 * i + 3 + axis])) / (2 * h)
-                lhs += float(g[c, 9 * mm + 2 * rows + 2 * i + axis]) * d
-    rhs = float((mg * vm).sum() + (ng * vn).sum())
+                out += float(g[c, 9 * mm + 2 * rows + 2 * i + axis]) * (float(la[ro + 6 * i + 3 + axis]) -
+                                                                        float(lb[ro + 6 * i + 3 + axis]))
+        return out
+
+    # Central differences over all creatures; for the start positions alone,
+    # which are piecewise linear in the genes, only creatures where the
+    # packer has no kink within [-h, h] along the direction (its one-sided
+    # differences agree: no muscle's length crosses its span, no other node
+    # becomes the lowest).
+    lhs = rhs = 0.0
+    kept = 0
+    for c in range(len(wave)):
+        up, down = record_change(wp, wave, c) / h, record_change(wave, wm, c) / h
+        if part == "start" and abs(up - down) > 0.02 * max(abs(up), abs(down)) + 1e-4:
+            continue
+        kept += 1
+        gs = pop.genomes[int(wave.slots[c])]
+        ms, ns = slice(gs["muscle_start"], gs["muscle_start"] + gs["muscle_count"]), slice(
+            gs["node_start"], gs["node_start"] + gs["node_count"])
+        lhs += 0.5 * (up + down)
+        rhs += float((mg[ms] * vm[ms]).sum() + (ng[ns] * vn[ns]).sum())
+    assert kept >= 0.8 * len(wave), kept
     assert abs(lhs - rhs) <= 2e-3 * max(abs(rhs), 1.0), (lhs, rhs)
 
 
-@pytest.mark.parametrize("field", range(11))
-def test_fp64_tangent_matches_fp64_differences(field):
+@pytest.mark.parametrize("workload,field", [("gradients", f) for f in range(11)] +
+                         [("refine", f) for f in (0, 2, 4, 8, 9, 10)])
+def test_fp64_tangent_matches_fp64_differences(workload, field):
     """One record field of muscle 0 (field < 9), the friction of node 1
     (field 9) or the mass of node 1 (field 10, with 1 / total mass moving
-    along) of 8 creatures, 0.2 s trials."""
+    along) of 8 creatures, 0.2 s trials, in the calm world and in the
+    refined-search world (rough ground, hurdles, tremors, water, ice, wind,
+    thick air)."""
     from oracle.ref import Oracle
     o = Oracle()
-    w = WORKLOADS["gradients"]
+    w = WORKLOADS[workload]
     world = w.world(duration=0.2)
     pop = ce.generate(w.spec, 8)
     wave = ce.pack(pop, world)
     p, flags = ce.make_params(world), ce.world_flags(world)
-    rows, mm = 12, 20
+    rows, mm = int((wave.heads[:, 0] & 255).max()), int(wave.heads[:, 1].max())
     n = len(wave)
     dm = np.zeros((n, mm, 9))
     dn = np.zeros((n, rows))
