@@ -20,6 +20,14 @@ engine's launch shape is first tuned on a sample of the workload.
 With --adjoint it runs the gradient path instead: one checkpointed forward
 run (ce_forward) and one backward run (ce_backward) of the workload, and
 prints both GPU times and the gradients per second.
+
+With --refine it runs one gradient-refined search generation (refine.py):
+--creatures samples of --parents parents, the --elites best refined by
+--steps adjoint ascent steps, against plain resampling of the same elites
+for the same GPU time, and prints the fitness gained per GPU-second of both.
+
+    python -m evolution_simulator_gpu_b200.profile_case --workload refine \
+        --refine --creatures 1000000 --parents 1024 --elites 16384 --steps 5 --seconds 20
 """
 from __future__ import annotations
 
@@ -44,11 +52,26 @@ def main() -> None:
     ap.add_argument("--autotune", action="store_true", help="tune the launch shape on a sample first")
     ap.add_argument("--sample", type=int, default=262_144, help="creatures in the autotune sample")
     ap.add_argument("--adjoint", action="store_true", help="time forward + backward of the gradient path")
+    ap.add_argument("--refine", action="store_true", help="one gradient-refined search generation")
+    ap.add_argument("--parents", type=int, default=1024)
+    ap.add_argument("--elites", type=int, default=16_384)
+    ap.add_argument("--steps", type=int, default=5)
     args = ap.parse_args()
     if args.generations:
         return generations(args)
     if args.adjoint:
         return adjoint(args)
+    if args.refine:
+        import evolution_simulator_gpu_b200 as ce
+        from evolution_simulator_gpu_b200 import refine
+        from evolution_simulator_gpu_b200.configs import WORKLOADS
+        w = WORKLOADS[args.workload]
+        with ce.Engine(0) as eng:
+            out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
+                                count=args.creatures, elites=args.elites, steps=args.steps)
+        out.update(workload=args.workload, seconds=args.seconds)
+        print(json.dumps(out))
+        return
     import evolution_simulator_gpu_b200 as ce
     from evolution_simulator_gpu_b200.configs import WORKLOADS
     w = WORKLOADS[args.workload]

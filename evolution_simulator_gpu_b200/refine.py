@@ -1,0 +1,250 @@
+"""Gradient-refined search generation: Gaussian samples of parent genomes,
+one batched evaluation, adjoint gradient ascent on the best samples, and
+plain resampling of the same elites for the same GPU time as the yardstick.
+
+The samples move the optimizer's parameter vector of a body
+(src/qd.rs:2700-2770, `parameters` / `write_parameters`): per node x, y,
+diameter and friction; per bone rest length, joint range and organ; one log
+period shared by the muscles; per muscle the anchors, short and long length,
+phase, duty, log stiffness and reset phase. Coordinates go back to genes as
+`apply_parameters` does (src/qd.rs:2773-2811: y at least 0, rest length in
+[0.03, max bone], joint range within +-JOINT_LIMIT on its side, organ mass at
+least 0 and its place in [0, 1], the period scaled by exp(log period) / the
+first muscle's period within [min period, 10] s, anchors in [0, 1], short in
+[0.01, 0.8 max stroke], long in [short, max stroke], phase and reset wrapped,
+duty in [0.05, 0.95], stiffness exp(.) in [1, 120]), then the diameter and
+friction are held to the workload's ranges as `repair` holds them to the
+configured ones (src/evolution.rs:1230-1234). The topology never changes, so
+the rest of `repair` has nothing to do. The samples carry the muscles'
+strength factors of their parents unchanged (the parameter vector has none).
+
+The ascent moves the coordinates the adjoint differentiates: per muscle short,
+long, strength factor, phase and duty (phase = frac(-t_on / period), duty =
+(t_off - t_on) / period), per node friction. A step adds, per coordinate,
+`step` x gradient clipped to the coordinate's unit step of the optimizer's
+layout (src/qd.rs:2620-2660: 0.02 x the body's mean bone length for lengths,
+0.05 for phase and duty, 0.03 for friction; 0.05 for the strength factor),
+then applies the same clamps. A creature keeps the best fitness it reached.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import api
+
+MAX_BONE = 2.0            # physics::Limits::DEFAULT.max_bone (src/physics.rs:142-153)
+MAX_STROKE = 2.0          # .max_stroke
+MIN_PERIOD = 0.2          # .min_period
+JOINT_LIMIT = float(np.float32(120.0 * np.pi / 180.0))  # src/evolution.rs:92
+DIAMETER = (0.06, 0.12)   # the workloads' node diameters
+FRICTION = (0.0, 1.0)     # the workloads' node friction
+STRENGTH = (0.5, 1.5)     # the workloads' strength factors
+UNIT = dict(length=0.02, phase=0.05, duty=0.05, friction=0.03, strength=0.05)
+
+
+def take(pop: api.Population, idx, ids=None) -> api.Population:
+    """The creatures `idx` of `pop` (repeats allowed) as a population of
+    their own, in that order, with genome ids `ids` (theirs by default)."""
+    idx = np.asarray(idx, np.int64)
+    g = pop.genomes[idx]
+
+    def gather(start, count, arr):
+        cnt = g[count].astype(np.int64)
+        out_start = np.cumsum(cnt) - cnt
+        src = np.repeat(g[start].astype(np.int64) - out_start, cnt) + np.arange(int(cnt.sum()))
+        # Rows as plain 32-bit words: fancy indexing of a structured array
+        # is several times slower.
+        words = arr.view(np.uint32).reshape(len(arr), arr.dtype.itemsize // 4)
+        return words[src].reshape(-1).view(arr.dtype), out_start, cnt, src
+
+    nodes, ns, nc, _ = gather("node_start", "node_count", pop.nodes)
+    bones, bs, bc, _ = gather("bone_start", "bone_count", pop.bones)
+    muscles, ms, mc, msrc = gather("muscle_start", "muscle_count", pop.muscles)
+    strength = None if pop.strength is None else pop.strength[msrc].copy()
+    genomes = np.zeros(len(idx), api.GENOME_DTYPE)
+    genomes["node_start"], genomes["node_count"] = ns, nc
+    genomes["bone_start"], genomes["bone_count"] = bs, bc
+    genomes["muscle_start"], genomes["muscle_count"] = ms, mc
+    genomes["id"] = g["id"] if ids is None else np.asarray(ids, np.uint64)
+    genomes["flags"] = g["flags"]
+    return api.Population(nodes, bones, muscles, genomes, strength)
+
+
+def _owner(pop: api.Population, start: str, count: str) -> np.ndarray:
+    """The creature of each node, bone or muscle row."""
+    return np.repeat(np.arange(len(pop.genomes)), pop.genomes[count].astype(np.int64))
+
+
+def _size(pop: api.Population) -> np.ndarray:
+    """Each creature's mean bone rest length within [0.05, 10] (1 without
+    bones): the optimizer layout's length unit (src/qd.rs:2641-2655)."""
+    owner = _owner(pop, "bone_start", "bone_count")
+    total = np.bincount(owner, pop.bones["rest_length"].astype(np.float64), len(pop.genomes))
+    cnt = pop.genomes["bone_count"].astype(np.float64)
+    size = np.where(cnt > 0, total / np.maximum(cnt, 1.0), 1.0)
+    return np.clip(size, 0.05, 10.0).astype(np.float32)
+
+
+def samples(parents: api.Population, count: int, sigma: float, seed: int, first_id: int = 1):
+    """`count` samples, sample i a child of parent i mod len(parents) with
+    every parameter-vector coordinate moved by sigma x N(0, 1) (seeded), ids
+    first_id + i. Returns (population, parent of each sample)."""
+    parent = np.arange(count, dtype=np.int64) % len(parents)
+    pop = take(parents, parent, first_id + np.arange(count, dtype=np.uint64))
+    rng = np.random.default_rng(seed)
+    f32 = np.float32
+
+    def noise(n):
+        return f32(sigma) * rng.standard_normal(n, dtype=f32)
+
+    n = pop.nodes
+    n["x"] += noise(len(n))
+    n["y"] = np.maximum(n["y"] + noise(len(n)), f32(0.0))
+    n["diameter"] = np.clip(n["diameter"] + noise(len(n)), *DIAMETER)
+    n["friction"] = np.clip(n["friction"] + noise(len(n)), *FRICTION)
+    b = pop.bones
+    b["rest_length"] = np.clip(b["rest_length"] + noise(len(b)), f32(0.03), f32(MAX_BONE))
+    b["min_angle"] = np.clip(b["min_angle"] + noise(len(b)), f32(-JOINT_LIMIT), f32(0.0))
+    b["max_angle"] = np.clip(b["max_angle"] + noise(len(b)), f32(0.0), f32(JOINT_LIMIT))
+    b["organ_mass"] = np.maximum(b["organ_mass"] + noise(len(b)), f32(0.0))
+    b["organ_at"] = np.clip(b["organ_at"] + noise(len(b)), f32(0.0), f32(1.0))
+    m = pop.muscles
+    owner = _owner(pop, "muscle_start", "muscle_count")
+    first = pop.genomes["muscle_start"].astype(np.int64)
+    has = pop.genomes["muscle_count"] > 0
+    base = np.ones(count, f32)
+    base[has] = np.maximum(m["period"][first[has]], f32(1e-3))
+    log_period = np.log(base) + noise(count)
+    scale = np.clip(np.exp(log_period), f32(MIN_PERIOD), f32(10.0)) / base
+    m["anchor_a"] = np.clip(m["anchor_a"] + noise(len(m)), f32(0.0), f32(1.0))
+    m["anchor_b"] = np.clip(m["anchor_b"] + noise(len(m)), f32(0.0), f32(1.0))
+    m["short"] = np.clip(m["short"] + noise(len(m)), f32(0.01), f32(0.8 * MAX_STROKE))
+    m["long"] = np.clip(m["long"] + noise(len(m)), m["short"], f32(MAX_STROKE))
+    m["period"] = np.clip(m["period"] * scale[owner], f32(MIN_PERIOD), f32(10.0))
+    m["phase"] = np.mod(m["phase"] + noise(len(m)), f32(1.0))
+    m["duty"] = np.clip(m["duty"] + noise(len(m)), f32(0.05), f32(0.95))
+    m["stiffness"] = np.clip(np.exp(np.log(np.maximum(m["stiffness"], f32(1e-3))) + noise(len(m))), f32(1.0),
+                             f32(120.0))
+    m["reset"] = np.mod(m["reset"] + noise(len(m)), f32(1.0))
+    return pop, parent
+
+
+def ascend(pop: api.Population, muscle_grads: np.ndarray, node_grads: np.ndarray, step: float) -> api.Population:
+    """One clipped gradient-ascent step on the differentiated coordinates
+    (see the module docstring), from gene gradients (gene_gradients: per
+    muscle d/d short, long, strength factor, t_on, t_off; per node d/d
+    friction). Returns a new population."""
+    out = api.Population(pop.nodes.copy(), pop.bones.copy(), pop.muscles.copy(), pop.genomes.copy(),
+                         None if pop.strength is None else pop.strength.copy())
+    f32 = np.float32
+    gm = np.nan_to_num(np.asarray(muscle_grads, np.float64), nan=0.0, posinf=0.0, neginf=0.0)
+    gn = np.nan_to_num(np.asarray(node_grads, np.float64), nan=0.0, posinf=0.0, neginf=0.0)
+    m = out.muscles
+    T = m["period"].astype(np.float64)
+    length_unit = (UNIT["length"] * _size(out)[_owner(out, "muscle_start", "muscle_count")]).astype(np.float64)
+
+    def move(g, unit):
+        return np.clip(step * g, -unit, unit).astype(f32)
+
+    m["short"] = np.clip(m["short"] + move(gm[:, 0], length_unit), f32(0.01), f32(0.8 * MAX_STROKE))
+    m["long"] = np.clip(m["long"] + move(gm[:, 1], length_unit), m["short"], f32(MAX_STROKE))
+    m["phase"] = np.mod(m["phase"] + move(-T * (gm[:, 3] + gm[:, 4]), UNIT["phase"]), f32(1.0))
+    m["duty"] = np.clip(m["duty"] + move(T * gm[:, 4], UNIT["duty"]), f32(0.05), f32(0.95))
+    if out.strength is not None:
+        out.strength[:] = np.clip(out.strength + move(gm[:, 2], UNIT["strength"]), *STRENGTH)
+    out.nodes["friction"] = np.clip(out.nodes["friction"] + move(gn, UNIT["friction"]), *FRICTION)
+    return out
+
+
+def _fitness(wave: api.WavePack, results: np.ndarray) -> np.ndarray:
+    """Fitness in population order from results in packed order."""
+    out = np.empty(len(wave), np.float32)
+    out[wave.slots] = results["fitness"]
+    return out
+
+
+def _evaluate(engine, pop, world, chunk: int):
+    """(fitness in population order, GPU-busy seconds), in chunks."""
+    fit = np.empty(len(pop), np.float32)
+    busy = 0.0
+    for lo in range(0, len(pop), chunk):
+        part = take(pop, np.arange(lo, min(lo + chunk, len(pop))))
+        wave = api.pack(part, world)
+        res, secs = engine.run(wave, world)
+        fit[lo:lo + len(part)] = _fitness(wave, res)
+        busy += secs
+    return fit, busy
+
+
+def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
+           elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
+           resample: bool = True) -> dict:
+    """One gradient-refined search generation and its resampling yardstick.
+
+    1. `count` samples of `parents` parents (σ = sigma), evaluated in one
+       batch; 2. the `elites` best get `steps` ascent steps, each a
+       checkpointed forward run (which also scores the current genes) and a
+       backward run, then a last evaluation; 3. plain resampling gives the
+       same elites children (σ = sigma) for about the same GPU time, each
+       elite keeping the best of itself and its children. Fitness gained is
+       the elites' mean best fitness minus their mean sampled fitness; GPU
+       seconds are the kernels' device time (host packing not included)."""
+    report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step)
+    t0 = time.perf_counter()
+    base = api.generate(spec, parents)
+    pop, _ = samples(base, count, sigma, seed)
+    report["host_sample_s"] = time.perf_counter() - t0
+    fit, busy = _evaluate(engine, pop, world, chunk)
+    report["sample_gpu_s"] = busy
+    order = np.argsort(-np.where(np.isfinite(fit) & (fit > -1e19), fit, -np.inf), kind="stable")
+    top = order[:elites]
+    elite = take(pop, top)
+    f0 = fit[top].astype(np.float64)
+    report["elite_mean_fitness"] = float(f0.mean())
+    # Gradient refinement.
+    best = f0.copy()
+    x = elite
+    refine_s = 0.0
+    t0 = time.perf_counter()
+    first_equal = None
+    for k in range(steps):
+        wave = api.pack(x, world)
+        with engine.forward(wave, world) as tape:
+            fk = _fitness(wave, tape.results).astype(np.float64)
+            g = tape.backward()
+            shape = tape.shape
+            fwd, bwd = tape.seconds
+        refine_s += fwd + bwd
+        if k == 0:
+            # The elites' genes, scored again by the checkpointed forward run.
+            first_equal = bool(np.array_equal(fk, f0))
+        best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+        mg, ng = api.gene_gradients(x, wave, world, g, shape)
+        x = ascend(x, mg, ng, step)
+    fk, secs = _evaluate(engine, x, world, chunk)
+    refine_s += secs
+    best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+    gain = float((best - f0).mean())
+    report["refine"] = dict(first_equal=first_equal, gpu_s=refine_s, mean_best=float(best.mean()), gain=gain, gain_per_gpu_s=gain / refine_s,
+                            improved=float((best > f0).mean()), host_s=time.perf_counter() - t0)
+    if resample:
+        per = max(1, int(round(refine_s / (report["sample_gpu_s"] / count) / elites)))
+        t0 = time.perf_counter()
+        bestr = f0.copy()
+        secs = 0.0
+        rounds = max(1, chunk // elites)
+        for r0 in range(0, per, rounds):
+            n = min(rounds, per - r0) * elites
+            kids, parent = samples(elite, n, sigma, seed + 1 + r0)
+            # Children keep their elite's id, so they see its tremor phase.
+            kids.genomes["id"] = elite.genomes["id"][parent]
+            fk, busy = _evaluate(engine, kids, world, chunk)
+            secs += busy
+            np.maximum.at(bestr, parent, np.where(fk > -1e19, fk, -np.inf).astype(np.float64))
+        gain_r = float((bestr - f0).mean())
+        report["resample"] = dict(children_per_elite=per, gpu_s=secs, mean_best=float(bestr.mean()), gain=gain_r,
+                                  gain_per_gpu_s=gain_r / secs, improved=float((bestr > f0).mean()),
+                                  host_s=time.perf_counter() - t0)
+    return report

@@ -76,14 +76,16 @@ def test_adjoint_matches_fp64_tangent(engine, name, seconds, median, share):
     assert (rel < 1e-3).mean() >= share, (rel < 1e-3).mean()
 
 
-@pytest.mark.parametrize("name", ["gradients", "refine"])
-def test_gene_gradients_match_fp64_differences(engine, name):
+@pytest.mark.parametrize("name,count", [("gradients", 64), ("refine", 192)])
+def test_gene_gradients_match_fp64_differences(engine, name, count):
     """End to end: GPU record gradient, gene chain rule, against central
     differences of the FP64 host physics over repacked genes (h = 2e-4,
-    mode-preserving perturbations: the one-sided differences agree)."""
+    mode-preserving perturbations: the one-sided differences agree; in the
+    effects world fewer creatures keep every contact, ice and water mode
+    over the step, so more are drawn)."""
     w = WORKLOADS[name]
     world = w.world(duration=0.1)
-    pop = ce.generate(w.spec, 64)
+    pop = ce.generate(w.spec, count)
     wave = ce.pack(pop, world)
     with engine.forward(wave, world) as tape:
         g = tape.backward()
