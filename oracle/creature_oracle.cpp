@@ -91,6 +91,7 @@ struct Sim {
     };
     T fit_t = T(0.0f);  // the fitness as a T (its derivative parts for a dual T)
     const double* seed_mass = nullptr;  // dual T: node-mass directions set in begin
+    const double* seed_start = nullptr; // dual T: start-position directions (x, y a node) set in begin
     // Checkpoints of another run of the same trial (positions, velocities,
     // energy stores every `resync_every` substeps, rows x 4 + mm floats
     // each): when set, the state's values are reset to them at each
@@ -233,6 +234,10 @@ struct Sim {
             node[i] = Node{m, T(1.0f) / m, T(fbits(r[1])), T(fbits(r[2]))};
             px[i] = T(fbits(r[3]));
             py[i] = T(fbits(r[4]));
+            if (seed_start) {
+                set_deriv(px[i], seed_start[2 * i]);
+                set_deriv(py[i], seed_start[2 * i + 1]);
+            }
             feet |= (r[5] & 1u) << i;
         }
         if (seed_mass) {
@@ -788,9 +793,10 @@ void simulate(const uint32_t* records, const float* muscles, const uint32_t* hea
 double tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t cidx, const Params& p,
                uint32_t flags, int rate, const double* dmuscle, const double* dnode, Result* out,
                const float* resync, uint32_t rows, uint32_t mm, uint32_t count, uint32_t every, double* fitness,
-               const double* dmass) {
+               const double* dmass, const double* dstart) {
     Sim<Dual> s(p, flags, rate);
     s.seed_mass = dmass;
+    s.seed_start = dstart;
     s.begin(records, muscles, heads, cidx);
     s.resync_every = every > 0 ? every : 256u;
     s.resync = resync;
@@ -863,19 +869,20 @@ void oracle_trace(const uint32_t* records, const float* muscles, const uint32_t*
 // FP64 tangents of creatures [first, first + n): for creature c the record
 // directions sit at dmuscle + c * 9 * mm and dnode + c * rows; d fitness goes
 // to dfit[c] and the FP64 fitness to fit[c] (when not NULL). `dmass` (NULL
-// for none, else rows a creature) moves the node masses too. Returns the wall
-// seconds.
+// for none, else rows a creature) moves the node masses too, and `dstart`
+// (NULL for none, else 2 x rows a creature) the start positions. Returns the
+// wall seconds.
 double oracle_tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t first, size_t n,
                       const oracle::Params* p, uint32_t flags, int rate, const double* dmuscle, const double* dnode,
                       uint32_t rows, uint32_t mm, double* dfit, double* fit, oracle::Result* out, int threads,
-                      const double* dmass) {
+                      const double* dmass, const double* dstart) {
     if (threads > 0) omp_set_num_threads(threads);
     const auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 1)
     for (long long i = 0; i < (long long)n; i++) {
         dfit[i] = oracle::tangent(records, muscles, heads, first + i, *p, flags, rate, dmuscle + i * 9 * mm,
                                   dnode + i * rows, out + i, nullptr, 0, 0, 0, 256, fit ? fit + i : nullptr,
-                                  dmass ? dmass + i * rows : nullptr);
+                                  dmass ? dmass + i * rows : nullptr, dstart ? dstart + 2 * i * rows : nullptr);
     }
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -895,7 +902,7 @@ double oracle_tangent_along(const uint32_t* records, const float* muscles, const
     for (long long i = 0; i < (long long)n; i++) {
         dfit[i] = oracle::tangent(records, muscles, heads, first + i, *p, flags, rate, dmuscle + i * 9 * mm,
                                   dnode + i * rows, out + i, ckpt + (first + i) * ckpt_stride, rows, mm, count,
-                                  every, fit ? fit + i : nullptr, dmass ? dmass + i * rows : nullptr);
+                                  every, fit ? fit + i : nullptr, dmass ? dmass + i * rows : nullptr, nullptr);
     }
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }

@@ -164,7 +164,7 @@ void simulate(const uint32_t* records, const float* muscles, const uint32_t* hea
 double tangent(const uint32_t* records, const float* muscles, const uint32_t* heads, size_t cidx, const Params& p,
                uint32_t flags, int rate, const double* dmuscle, const double* dnode, Result* out,
                const float* resync, uint32_t rows, uint32_t mm, uint32_t count, uint32_t every,
-               double* fitness, const double* dmass);
+               double* fitness, const double* dmass, const double* dstart = nullptr);
 
 // The value part of a scalar of the oracle (for dual numbers: keeps the
 // derivative).

@@ -90,7 +90,7 @@ class Oracle:
         self.lib.oracle_tangent.restype = C.c_double
         self.lib.oracle_tangent.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p,
                                             C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
-                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         self.lib.oracle_tangent_along.restype = C.c_double
         self.lib.oracle_tangent_along.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t,
                                                   C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p,
@@ -128,12 +128,13 @@ class Oracle:
         return out[0], counts
 
     def tangent(self, wave, params, flags: int, dmuscle, dnode, rate: int = 60, first: int = 0, threads: int = 0,
-                dmass=None):
+                dmass=None, dstart=None):
         """FP64 forward-mode tangents of the fitness of packed creatures
         [first, first + n): creature c's record fields move along
         dmuscle[c] (muscle slots x 9: amplitude, hill, cap, 1/capacity, phase,
         duty, 1/duty, 1/(1-duty), stiffness) and dnode[c] (node rows:
-        friction) and dmass[c] (node rows: mass; None for none). Returns
+        friction) and dmass[c] (node rows: mass; None for none) and
+        dstart[c] (node rows x 2: start x, y; None for none). Returns
         (d fitness [n], FP64 results, wall seconds); the FP64 fitness itself
         is left in `self.fitness64`."""
         dm = np.ascontiguousarray(dmuscle, np.float64)
@@ -146,7 +147,8 @@ class Oracle:
         secs = self.lib.oracle_tangent(wave.lanes.ctypes.data, wave.muscles.ctypes.data, wave.heads.ctypes.data,
                                        first, n, C.byref(params), flags, rate, dm.ctypes.data, dn.ctypes.data, rows,
                                        mm, dfit.ctypes.data, fit.ctypes.data, out.ctypes.data, threads,
-                                       None if dmass is None else np.ascontiguousarray(dmass, np.float64).ctypes.data)
+                                       None if dmass is None else np.ascontiguousarray(dmass, np.float64).ctypes.data,
+                                       None if dstart is None else np.ascontiguousarray(dstart, np.float64).ctypes.data)
         self.fitness64 = fit
         return dfit, out, secs
 

@@ -24,22 +24,33 @@ W = WORKLOADS["gradients"]
 R = WORKLOADS["refine"]
 
 
-def _record_direction(wave, rows, mm, rng):
-    dm = rng.normal(size=(len(wave), mm, 9))
-    dn = rng.normal(size=(len(wave), rows))
-    dmass = rng.normal(size=(len(wave), rows)) * 0.01
-    for c in range(len(wave)):
+def _record_direction(wave, rows, mm, rng, part="records"):
+    """A random direction in the record fields (muscle fields, friction,
+    mass) or in the start positions alone."""
+    n = len(wave)
+    dm = rng.normal(size=(n, mm, 9))
+    dn = rng.normal(size=(n, rows))
+    dmass = rng.normal(size=(n, rows)) * 0.01
+    ds = rng.normal(size=(n, rows, 2))
+    if part == "records":
+        ds[:] = 0.0
+    else:
+        dm[:], dn[:], dmass[:] = 0.0, 0.0, 0.0
+    for c in range(n):
+        nodes = int(wave.heads[c, 0] & 255)
         dm[c, int(wave.heads[c, 1]):] = 0.0
-        dn[c, int(wave.heads[c, 0] & 255):] = 0.0
-        dmass[c, int(wave.heads[c, 0] & 255):] = 0.0
-    return dm, dn, dmass
+        dn[c, nodes:] = 0.0
+        dmass[c, nodes:] = 0.0
+        ds[c, nodes:] = 0.0
+    return dm, dn, dmass, ds
 
 
-def _project(g, rows, mm, dm, dn, dmass):
+def _project(g, rows, mm, dm, dn, dmass, ds):
     g = g.astype(np.float64)
     n = len(g)
     return ((g[:, :9 * mm].reshape(n, mm, 9) * dm).sum(axis=(1, 2)) + (g[:, 9 * mm:9 * mm + rows] * dn).sum(axis=1)
-            + (g[:, 9 * mm + rows:9 * mm + 2 * rows] * dmass).sum(axis=1))
+            + (g[:, 9 * mm + rows:9 * mm + 2 * rows] * dmass).sum(axis=1)
+            + (g[:, 9 * mm + 2 * rows:9 * mm + 4 * rows] * ds.reshape(n, 2 * rows)).sum(axis=1))
 
 
 @pytest.mark.parametrize("name,quake", [("gradients", True), ("refine", True), ("refine", False)])
@@ -53,13 +64,15 @@ def test_forward_results_equal_the_plain_kernel(engine, name, quake):
     assert (res.view(np.uint32) == plain.view(np.uint32)).all()
 
 
-@pytest.mark.parametrize("name,seconds,median,share", [("gradients", 0.05, 1e-4, 0.95), ("gradients", 0.25, 1e-3, 0.55),
-                                                       ("refine", 0.05, 1e-4, 0.9), ("refine", 0.25, 1e-3, 0.5)])
-def test_adjoint_matches_fp64_tangent(engine, name, seconds, median, share):
+@pytest.mark.parametrize("name,part,seconds,median,share", [
+    ("gradients", "records", 0.05, 1e-4, 0.95), ("gradients", "records", 0.25, 1e-3, 0.55),
+    ("refine", "records", 0.05, 1e-4, 0.9), ("refine", "records", 0.25, 1e-3, 0.5),
+    ("gradients", "start", 0.1, 1e-4, 0.9), ("refine", "start", 0.1, 1e-4, 0.9)])
+def test_adjoint_matches_fp64_tangent(engine, name, part, seconds, median, share):
     """<gradient, u> against the FP64 tangent along u for 256 creatures, u a
-    random direction in all record fields (muscles, friction, mass), in the
-    calm world and in the refined-search world (rough ground with hurdles and
-    tremors, water, ice, wind, thick air)."""
+    random direction in the record fields (muscles, friction, mass) or in the
+    start positions, in the calm world and in the refined-search world
+    (rough ground with hurdles and tremors, water, ice, wind, thick air)."""
     w = WORKLOADS[name]
     world = w.world(duration=seconds)
     wave = ce.pack(ce.generate(w.spec, 256), world)
@@ -67,24 +80,50 @@ def test_adjoint_matches_fp64_tangent(engine, name, seconds, median, share):
         g = tape.backward()
         rows, mm = tape.shape
         res = tape.results
-    dm, dn, dmass = _record_direction(wave, rows, mm, np.random.default_rng(7))
-    tangent, _, _ = Oracle().tangent(wave, ce.make_params(world), ce.world_flags(world), dm, dn, dmass=dmass)
-    adj = _project(g, rows, mm, dm, dn, dmass)
+    dm, dn, dmass, ds = _record_direction(wave, rows, mm, np.random.default_rng(7), part)
+    tangent, _, _ = Oracle().tangent(wave, ce.make_params(world), ce.world_flags(world), dm, dn, dmass=dmass,
+                                     dstart=ds)
+    adj = _project(g, rows, mm, dm, dn, dmass, ds)
     ok = res["fitness"] > -1e19
     rel = np.abs(adj - tangent)[ok] / np.maximum(np.abs(tangent[ok]), 1e-12)
     assert np.median(rel) < median, np.median(rel)
     assert (rel < 1e-3).mean() >= share, (rel < 1e-3).mean()
 
 
-@pytest.mark.parametrize("name,count", [("gradients", 64), ("refine", 192)])
-def test_gene_gradients_match_fp64_differences(engine, name, count):
+# Record float index of each gradient field of a muscle (kernel record layout).
+FIELDS = [8, 3, 4, 5, 10, 11, 12, 13, 14]
+
+
+def _record_change(wa, wb, h):
+    """d records / d h of a one-creature pack by central differences: the
+    gradient's record fields (muscle fields, friction, mass, start x and y)
+    as (muscle, node, mass, start) direction arrays for the FP64 tangent."""
+    M, N = int(wa.heads[0, 1]), int(wa.heads[0, 0] & 255)
+    mo, ro = int(wa.heads[0, 4]), int(wa.heads[0, 3])
+    la, lb = wa.lanes.view(np.float32).astype(np.float64), wb.lanes.view(np.float32).astype(np.float64)
+    ma, mb = wa.muscles.astype(np.float64), wb.muscles.astype(np.float64)
+    dm = np.zeros((1, M, 9))
+    for k in range(M):
+        dm[0, k] = (ma[mo + 20 * k + np.array(FIELDS)] - mb[mo + 20 * k + np.array(FIELDS)]) / (2 * h)
+    rows = ro + 6 * np.arange(N)
+    dn = ((la[rows + 2] - lb[rows + 2]) / (2 * h))[None]
+    dmass = ((la[rows] - lb[rows]) / (2 * h))[None]
+    ds = np.stack([(la[rows + 3] - lb[rows + 3]) / (2 * h), (la[rows + 4] - lb[rows + 4]) / (2 * h)], 1)[None]
+    return dm, dn, dmass, ds
+
+
+@pytest.mark.parametrize("name,count,seconds", [("gradients", 64, 0.1), ("refine", 384, 0.05)])
+def test_gene_gradients_match_fp64_differences(engine, name, count, seconds):
     """End to end: GPU record gradient, gene chain rule, against central
-    differences of the FP64 host physics over repacked genes (h = 2e-4,
-    mode-preserving perturbations: the one-sided differences agree; in the
-    effects world fewer creatures keep every contact, ice and water mode
-    over the step, so more are drawn)."""
+    differences of the FP64 host physics over repacked genes (h = 2e-4),
+    where the FP64 fitness is differentiable at the genes: its one-sided
+    differences agree, and its FP64 tangent along the packer's record
+    change equals the central difference. The second test matters on uneven
+    ground, where the start pose rests its lowest node exactly on the
+    ground: whether a repacked pose touches there turns on rounding, and the
+    contact branch has other derivatives than the free one."""
     w = WORKLOADS[name]
-    world = w.world(duration=0.1)
+    world = w.world(duration=seconds)
     pop = ce.generate(w.spec, count)
     wave = ce.pack(pop, world)
     with engine.forward(wave, world) as tape:
@@ -105,7 +144,7 @@ def test_gene_gradients_match_fp64_differences(engine, name, count):
         kink = (m["duty"] <= 0.0501) | (m["duty"] >= 0.9499) | (m["phase"] < 0.01) | (m["phase"] > 0.99)
         vm[kink, 3:] = 0.0
 
-        def fitness(h):
+        def moved(h):
             mm_ = m.copy()
             nn = one.nodes.copy()
             T = mm_["period"].astype(np.float64)
@@ -115,22 +154,29 @@ def test_gene_gradients_match_fp64_differences(engine, name, count):
             mm_["duty"] = (mm_["duty"] + h * (vm[:, 4] - vm[:, 3]) / T).astype(np.float32)
             nn["friction"] = (nn["friction"] + h * vn).astype(np.float32)
             st = (one.strength + h * vm[:, 2]).astype(np.float32)
-            w1 = ce.pack(ce.Population(nn, one.bones, mm_, one.genomes, st), world)
+            return ce.pack(ce.Population(nn, one.bones, mm_, one.genomes, st), world)
+
+        def fitness(w1):
             o.tangent(w1, p, flags, np.zeros((1, int(w1.heads[0, 1]), 9)), np.zeros((1, int(w1.heads[0, 0] & 255))))
             return float(o.fitness64[0])
 
         h = 2e-4
-        f0, fp, fm = fitness(0.0), fitness(h), fitness(-h)
+        w0 = moved(0.0)
+        f0, fp, fm = fitness(w0), fitness(moved(h)), fitness(moved(-h))
         up, down = (fp - f0) / h, (f0 - fm) / h
         if abs(up - down) > 0.05 * max(abs(up), abs(down)) + 1e-9:
             continue
         fd = (fp - fm) / (2 * h)
+        dm, dn, dmass, ds = _record_change(moved(1e-3), moved(-1e-3), 1e-3)
+        along, _, _ = o.tangent(w0, p, flags, dm, dn, dmass=dmass, dstart=ds)
+        if abs(float(along[0]) - fd) > 2e-2 * max(abs(fd), 1e-6):
+            continue
         gs = pop.genomes[i]
         got = float((mg[gs["muscle_start"]:gs["muscle_start"] + gs["muscle_count"]] * vm).sum()
                     + (ng[gs["node_start"]:gs["node_start"] + gs["node_count"]] * vn).sum())
         checked += 1
         agree += abs(got - fd) <= 2e-2 * max(abs(fd), 1e-6)
-    assert checked >= 24, checked
+    assert checked >= 20, checked
     assert agree >= 0.8 * checked, (agree, checked)
 
 

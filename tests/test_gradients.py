@@ -110,14 +110,14 @@ def test_gene_chain_rule_matches_packer_differences(workload, part):
     assert abs(lhs - rhs) <= 2e-3 * max(abs(rhs), 1.0), (lhs, rhs)
 
 
-@pytest.mark.parametrize("workload,field", [("gradients", f) for f in range(11)] +
-                         [("refine", f) for f in (0, 2, 4, 8, 9, 10)])
+@pytest.mark.parametrize("workload,field", [("gradients", f) for f in range(13)] +
+                         [("refine", f) for f in (0, 2, 4, 8, 9, 10, 11, 12)])
 def test_fp64_tangent_matches_fp64_differences(workload, field):
     """One record field of muscle 0 (field < 9), the friction of node 1
-    (field 9) or the mass of node 1 (field 10, with 1 / total mass moving
-    along) of 8 creatures, 0.2 s trials, in the calm world and in the
-    refined-search world (rough ground, hurdles, tremors, water, ice, wind,
-    thick air)."""
+    (field 9), the mass of node 1 (field 10, with 1 / total mass moving
+    along) or the start x or y of node 1 (fields 11, 12) of 8 creatures,
+    0.2 s trials, in the calm world and in the refined-search world (rough
+    ground, hurdles, tremors, water, ice, wind, thick air)."""
     from oracle.ref import Oracle
     o = Oracle()
     w = WORKLOADS[workload]
@@ -130,6 +130,7 @@ def test_fp64_tangent_matches_fp64_differences(workload, field):
     dm = np.zeros((n, mm, 9))
     dn = np.zeros((n, rows))
     dmass = np.zeros((n, rows))
+    dstart = np.zeros((n, rows, 2))
     lf = wave.lanes.view(np.float32)
     for c in range(n):
         mo, ro = int(wave.heads[c, 4]), int(wave.heads[c, 3])
@@ -137,9 +138,11 @@ def test_fp64_tangent_matches_fp64_differences(workload, field):
             dm[c, 0, field] = wave.muscles[mo + FIELDS[field]]
         elif field == 9:
             dn[c, 1] = lf[ro + 6 + 2]
-        else:
+        elif field == 10:
             dmass[c, 1] = lf[ro + 6]
-    tangent, _, _ = o.tangent(wave, p, flags, dm, dn, dmass=dmass)
+        else:
+            dstart[c, 1, field - 11] = 1.0
+    tangent, _, _ = o.tangent(wave, p, flags, dm, dn, dmass=dmass, dstart=dstart)
 
     def run(eps):
         mus = wave.muscles.copy()
@@ -152,6 +155,8 @@ def test_fp64_tangent_matches_fp64_differences(workload, field):
                 mus[mo + FIELDS[field]] = np.float32(wave.muscles[mo + FIELDS[field]] * (1 + eps))
             elif field == 9:
                 lf2[ro + 6 + 2] = np.float32(lf[ro + 6 + 2] * (1 + eps))
+            elif field > 10:
+                lf2[ro + 6 + 3 + field - 11] = np.float32(lf[ro + 6 + 3 + field - 11] + eps)
             else:
                 dmass_c = float(lf[ro + 6]) * eps
                 lf2[ro + 6] = np.float32(lf[ro + 6] + dmass_c)
@@ -161,7 +166,11 @@ def test_fp64_tangent_matches_fp64_differences(workload, field):
                   np.zeros_like(dn))
         return o.fitness64.copy()
 
-    h = 1e-3
+    # A start position moves by an absolute 2^-20 m (exact in float32 for
+    # positions below 8 m: the start pose rests a node exactly on the ground,
+    # so larger moves change its contact mode), the other fields by 1e-3
+    # relative.
+    h = 2.0 ** -20 if field > 10 else 1e-3
     f0, fp, fm = run(0.0), run(h), run(-h)
     fd = (fp - fm) / (2 * h)
     # Mode-preserving perturbations only: the one-sided differences agree
