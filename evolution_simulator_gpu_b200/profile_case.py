@@ -15,7 +15,10 @@ same batch and prints whether the results are equal to the bit.
 With --generations K it packs K generations of the workload (disjoint
 creature ranges), keeps them resident and runs them as one CUDA graph
 (GenerationGraph), once to warm up and once timed; with --autotune the
-engine's launch shape is first tuned on a sample of the workload.
+engine's launch shape is first tuned on a sample of the workload: by
+default a whole generation's worth of creatures on shorter trials
+(--sample-seconds), since the best shape depends on how many creatures
+share the GPU's lanes and how unevenly their trials end.
 
 With --adjoint it runs the gradient path instead: one checkpointed forward
 run (ce_forward) and one backward run (ce_backward) of the workload, and
@@ -50,7 +53,8 @@ def main() -> None:
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="resident blocks per SM (0: the engine's choice)")
     ap.add_argument("--generations", type=int, default=0, help="run K resident generations as one CUDA graph")
     ap.add_argument("--autotune", action="store_true", help="tune the launch shape on a sample first")
-    ap.add_argument("--sample", type=int, default=262_144, help="creatures in the autotune sample")
+    ap.add_argument("--sample", type=int, default=0, help="creatures in the autotune sample (0: --creatures)")
+    ap.add_argument("--sample-seconds", type=float, default=2.0, help="trial length of the autotune sample")
     ap.add_argument("--adjoint", action="store_true", help="time forward + backward of the gradient path")
     ap.add_argument("--refine", action="store_true", help="one gradient-refined search generation")
     ap.add_argument("--parents", type=int, default=1024)
@@ -124,8 +128,11 @@ def generations(args) -> None:
     out["record_bytes"] = int(sum(v.lanes.nbytes + v.muscles.nbytes + v.heads.nbytes for v in waves))
     with ce.Engine(0, ctas_per_sm=args.ctas_per_sm) as eng:
         if args.autotune:
-            sample = ce.pack(ce.generate(w.spec, args.sample, first=args.generations * args.creatures), world)
-            out["launch_shape"], out["autotune_best_s"] = eng.autotune(sample, world)
+            short = w.world(duration=args.sample_seconds)
+            sample = ce.pack(ce.generate(w.spec, args.sample or args.creatures, first=args.generations * args.creatures),
+                             short)
+            out["launch_shape"], out["autotune_best_s"] = eng.autotune(sample, short)
+            del sample
         with ce.GenerationGraph(eng, waves, world) as g:
             out["warm_s"] = g.launch()
             out["graph_s"] = g.launch()
