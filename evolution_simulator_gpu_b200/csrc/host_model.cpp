@@ -697,26 +697,52 @@ extern "C" uint32_t ce_frame_stride(uint32_t max_muscles) { return 2u * CE_MAX_N
 static bool pack_order(const ce_population* pop, const uint32_t* indices, size_t n,
                        std::vector<uint32_t>& sorted_slot) {
     sorted_slot.resize(n);
-    std::iota(sorted_slot.begin(), sorted_slot.end(), 0u);
-    auto idx = [&](uint32_t s) -> size_t { return indices ? indices[s] : s; };
-    for (size_t s = 0; s < n; s++) {
-        if (idx(s) >= pop->count) {
-            set_error("ce_pack: index out of range");
-            return false;
-        }
-        std::string why;
-        if (!validate_body(*pop, idx(s), &why)) {
-            set_error(why);
-            return false;
+    auto idx = [&](size_t s) -> size_t { return indices ? indices[s] : s; };
+    // Validation in parallel; the first failing slot's reason is kept.
+    long long bad = -1;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (long long s = 0; s < (long long)n; s++) {
+        if (idx((size_t)s) >= pop->count || !validate_body(*pop, idx((size_t)s), nullptr)) {
+#pragma omp critical(ce_pack_bad)
+            if (bad < 0 || s < bad) bad = s;
         }
     }
-    std::stable_sort(sorted_slot.begin(), sorted_slot.end(), [&](uint32_t x, uint32_t y) {
-        const ce_genome& a = pop->genomes[idx(x)];
-        const ce_genome& b = pop->genomes[idx(y)];
-        if (a.muscle_count != b.muscle_count) return a.muscle_count < b.muscle_count;
-        if (a.node_count != b.node_count) return a.node_count < b.node_count;
-        return idx(x) < idx(y);
-    });
+    if (bad >= 0) {
+        if (idx((size_t)bad) >= pop->count) {
+            set_error("ce_pack: index out of range");
+        } else {
+            std::string why;
+            validate_body(*pop, idx((size_t)bad), &why);
+            set_error(why);
+        }
+        return false;
+    }
+    // Order: muscle count, then node count, then population index. With the
+    // population indices ascending (or none given) a counting sort over the
+    // (muscles, nodes) key in slot order gives exactly that order.
+    bool ascending = true;
+    for (size_t s = 1; indices && s < n && ascending; s++) ascending = indices[s - 1] < indices[s];
+    if (!ascending) {
+        std::iota(sorted_slot.begin(), sorted_slot.end(), 0u);
+        std::stable_sort(sorted_slot.begin(), sorted_slot.end(), [&](uint32_t x, uint32_t y) {
+            const ce_genome& a = pop->genomes[idx(x)];
+            const ce_genome& b = pop->genomes[idx(y)];
+            if (a.muscle_count != b.muscle_count) return a.muscle_count < b.muscle_count;
+            if (a.node_count != b.node_count) return a.node_count < b.node_count;
+            return idx(x) < idx(y);
+        });
+        return true;
+    }
+    constexpr size_t kNodeKeys = CE_MAX_NODES + 1;
+    const size_t keys = (CE_MAX_MUSCLES + 1) * kNodeKeys;
+    std::vector<size_t> start(keys + 1, 0);
+    auto key = [&](size_t s) {
+        const ce_genome& g = pop->genomes[idx(s)];
+        return (size_t)g.muscle_count * kNodeKeys + g.node_count;
+    };
+    for (size_t s = 0; s < n; s++) start[key(s) + 1]++;
+    for (size_t k = 0; k < keys; k++) start[k + 1] += start[k];
+    for (size_t s = 0; s < n; s++) sorted_slot[start[key(s)]++] = (uint32_t)s;
     return true;
 }
 
