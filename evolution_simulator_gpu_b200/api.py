@@ -99,6 +99,11 @@ MUSCLE_DTYPE = np.dtype([("bone_a", "<u4"), ("bone_b", "<u4"), ("anchor_a", "<f4
                          ("short", "<f4"), ("long", "<f4"), ("period", "<f4"), ("phase", "<f4"),
                          ("duty", "<f4"), ("stiffness", "<f4"), ("sensor", "<u4"), ("reset", "<f4"),
                          ("tendon", "<f4")])
+DUMP_HEAD_DTYPE = np.dtype([("parent", "<u8"), ("slot", "<u4"), ("op", "<u2"), ("parent_cell", "<u2"),
+                            ("cma", "<u2"), ("period", "<u2"), ("emitter", "u1"), ("flags", "u1"), ("kind", "u1"),
+                            ("nodes", "u1"), ("muscles", "u1"), ("parent_nodes", "u1"), ("parent_muscles", "u1"),
+                            ("reserved", "u1")], align=True)
+DUMP_ROW_BYTES = 64
 GENOME_DTYPE = np.dtype([("node_start", "<u4"), ("node_count", "<u4"), ("bone_start", "<u4"),
                          ("bone_count", "<u4"), ("muscle_start", "<u4"), ("muscle_count", "<u4"),
                          ("id", "<u8"), ("flags", "<u4"), ("reserved", "<u4")])
@@ -184,6 +189,9 @@ def _bind(lib: C.CDLL) -> None:
         "ce_metrics_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_shape_classes": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
+        "ce_dump_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
+        "ce_dump_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World),
+                                          C.c_void_p, C.c_void_p]),
         "ce_height_bin_edges": (None, [C.c_void_p]),
         "ce_replay_decode": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -221,7 +229,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
-            "ce_replay_decode", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
+            "ce_replay_decode", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
             "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
 
 
@@ -567,7 +575,7 @@ class Engine:
         return forward(self, wave, world, checkpoint_every)
 
     def record(self, wave: WavePack, world: World):
-        """Every frame of each creature of `wave` (at most 64): an array
+        """Every frame of each creature of `wave` (at most 65,536): an array
         [creature, frame, slot, 2] in the reference's frame layout
         (src/creature_kernel.rs:312-326), and the results in packed order."""
         k = len(wave)
@@ -823,6 +831,28 @@ def metrics_device(results: int, heads: int, shapes: int, count: int, world: Wor
     of `count` results, equal to to_metrics and niche_cells to the bit."""
     _check(lib().ce_metrics_device(results, heads, shapes, count, C.byref(world), 1 if global_layout else 0,
                                    metrics or None, cells, stream or None), "ce_metrics_device")
+
+
+def dump_rows(results: np.ndarray, wave: WavePack, heads: np.ndarray, world: World,
+              archive_fitness: Optional[np.ndarray] = None) -> np.ndarray:
+    """The 64-byte generation dump rows (storage/dump.rs) of results in
+    packed order, on the host: a (count, 64) uint8 array."""
+    res = np.ascontiguousarray(results, RESULT_DTYPE)
+    dh = np.ascontiguousarray(heads, DUMP_HEAD_DTYPE)
+    af = None if archive_fitness is None else np.ascontiguousarray(archive_fitness, np.float32)
+    assert len(res) == len(wave) == len(dh)
+    out = np.zeros((len(res), DUMP_ROW_BYTES), np.uint8)
+    _check(lib().ce_dump_rows(_ptr(res), _ptr(wave.heads), _ptr(dh), _ptr(af), len(res), C.byref(world), _ptr(out)),
+           "ce_dump_rows")
+    return out
+
+
+def dump_rows_device(results: int, heads: int, dump_heads: int, archive_fitness: int, count: int, world: World,
+                     rows: int, stream: int = 0) -> None:
+    """dump_rows on device pointers (asynchronous on `stream`; `rows` 16-byte
+    aligned, `archive_fitness` 0 for the results' fitness)."""
+    _check(lib().ce_dump_rows_device(results, heads, dump_heads, archive_fitness or None, count, C.byref(world), rows,
+                                     stream or None), "ce_dump_rows_device")
 
 
 def ground(x: float, amplitude: float = 0.0, tilt: float = 0.0, width: float = 0.0, hurdle: float = 0.0,

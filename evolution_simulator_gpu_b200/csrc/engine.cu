@@ -493,8 +493,8 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     }
     ce_status s = check_world(w);
     if (s != CE_OK) return s;
-    if (pack->count > 64) {
-        set_error("ce_record: at most 64 creatures a recording");
+    if (pack->count > CE_RECORD_MAX_CREATURES) {
+        set_error("ce_record: at most " + std::to_string(CE_RECORD_MAX_CREATURES) + " creatures a recording");
         return CE_ERR_INVALID;
     }
     std::vector<ClassPlan> plans;
@@ -516,7 +516,9 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
         return CE_ERR_INVALID;
     }
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
-    const unsigned grid = 1;
+    // Frames are indexed by packed creature, so any grid records them; one
+    // block of lanes per 128 creatures, up to what the GPU holds at once.
+    const unsigned grid = grid_for(e, rows, mm, flags, true, rate, pack->count);
     const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
     const size_t res_b = pack->count * sizeof(ce_result);
     if ((s = e->rec_frames.ensure(frame_floats * 4)) || (s = e->rec_lanes.ensure(lanes_b)) ||

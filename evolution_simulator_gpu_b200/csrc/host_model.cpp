@@ -935,6 +935,57 @@ extern "C" ce_status ce_niche_batch(const ce_population* pop, const uint32_t* in
     return CE_OK;
 }
 
+static_assert(sizeof(ce_dump_head) == 32, "ce_dump_head is 32 bytes");
+
+// storage::dump::Dump::write_rows (src/storage/dump.rs:409-455) for
+// `count` results: the caller's heads, the behaviour cell (dump::cell,
+// storage/dump.rs:151-158) of each result's niche, its fitness and its rung
+// trace words.
+extern "C" ce_status ce_dump_rows(const ce_result* results, const uint32_t* heads, const ce_dump_head* dump,
+                                  const float* archive_fitness, size_t count, const ce_world* w, uint8_t* rows) {
+    if (!results || !heads || !dump || !w || !rows) {
+        set_error("ce_dump_rows: null argument");
+        return CE_ERR_INVALID;
+    }
+    for (size_t c = 0; c < count; c++) {
+        const ce_result& r = results[c];
+        const ce_dump_head& h = dump[c];
+        ce_metrics m;
+        ce_status s = ce_to_metrics(&r, heads[8 * c] & 255u, w, &m);
+        if (s != CE_OK) return s;
+        const uint8_t gc = qd_bin(clampf(m.ground_contact, 0.0f, 1.0f), 0.0f, 1.0f, 6);
+        const uint8_t gf = qd_bin(clampf(m.gait_frequency, 0.0f, 20.0f), 0.0f, 6.0f, 8);
+        const uint8_t hb = qd_bin(height_axis(fmax_(m.mean_height, 0.0f)), 0.0f, 1.0f, 6);
+        const float fr = std::round(fmax_(m.feet, 0.0f));
+        int32_t fi = fr >= 2147483647.0f ? 2147483647 : (fr <= -2147483648.0f ? (-2147483647 - 1) : (int32_t)fr);
+        fi = std::min(std::max(fi, 1), 5);
+        const uint16_t cell = (uint16_t)(((gc * 8u + gf) * 6u + hb) * 5u + (uint32_t)(fi - 1));
+        uint8_t* b = rows + (size_t)CE_DUMP_ROW_BYTES * c;
+        auto put = [&](size_t at, const void* v, size_t n) { std::memcpy(b + at, v, n); };
+        put(0, &h.slot, 4);
+        b[4] = h.emitter;
+        b[5] = (uint8_t)(h.op & 0xffu);
+        b[6] = (uint8_t)(h.flags | (m.screened ? CE_DUMP_SCREENED : 0u));
+        b[7] = (uint8_t)((h.kind & 15u) | (((h.op >> 8) & 15u) << 4));
+        put(8, &h.parent, 8);
+        put(16, &h.parent_cell, 2);
+        put(18, &cell, 2);
+        put(20, &h.cma, 2);
+        b[22] = h.nodes;
+        b[23] = h.muscles;
+        b[24] = h.parent_nodes;
+        b[25] = h.parent_muscles;
+        put(26, &h.period, 2);
+        put(28, &r.fitness, 4);
+        const float archive = archive_fitness ? archive_fitness[c] : r.fitness;
+        put(32, &archive, 4);
+        const float words[7] = {r.contact_hi,        r.lift_hi,           r.ground_hi, r.previous_center_y,
+                                r.vertical_extremum, r.vertical_trend,    r.gait_turns};
+        put(36, words, 28);
+    }
+    return CE_OK;
+}
+
 extern "C" void ce_ground(float x, float amplitude, float tilt, float width, float hurdle, float phase, float* height,
                           float* slope) {
     float h = 0.0f, sl = 0.0f;

@@ -255,6 +255,45 @@ typedef struct ce_metrics {
 ce_status ce_metrics_device(const ce_result* results, const uint32_t* heads, const uint8_t* shape_classes,
                             size_t count, const ce_world* world, int global_layout, ce_metrics* metrics,
                             int64_t* cells, void* stream);
+/* ---- generation dump rows (src/storage/dump.rs) ---- */
+/* One row a creature, 64 bytes little endian, in the layout of
+ * storage/dump.rs:76-113 (ROW_BYTES): the breeding fields the caller knows
+ * (ce_dump_head), the behaviour cell of the result
+ * (((contact * 8 + cadence) * 6 + height) * 5 + feet, dump::cell), the
+ * standard fitness, the archive fitness and the seven rung trace words of
+ * the result (GpuResult::rung_trace). The row's flags byte is the head's
+ * with CE_DUMP_SCREENED added when the screen stopped the trial
+ * (write_rows, storage/dump.rs:409-455). */
+#define CE_DUMP_ROW_BYTES 64u
+#define CE_DUMP_FINE 4u
+#define CE_DUMP_RERUN 8u
+#define CE_DUMP_SCREENED 16u
+#define CE_DUMP_EXCLUDED 32u
+#define CE_DUMP_PARENT_RESERVE 64u
+typedef struct ce_dump_head {
+    uint64_t parent;         /* parent id, UINT64_MAX for none */
+    uint32_t slot;           /* ring slot */
+    uint16_t op;             /* structural operator index (12 bits), 0xFFF for none */
+    uint16_t parent_cell;    /* parent's cell, UINT16_MAX for none */
+    uint16_t cma;            /* CMA emitter that sampled it, UINT16_MAX for none */
+    uint16_t period;         /* rhythm period of its first muscle, f16 bits */
+    uint8_t emitter;         /* Emitter::index */
+    uint8_t flags;           /* bred flags, with FINE, RERUN, EXCLUDED as the caller's metrics say */
+    uint8_t kind;            /* where the result entered (low four bits) */
+    uint8_t nodes, muscles, parent_nodes, parent_muscles;
+    uint8_t reserved;
+} ce_dump_head;
+/* Host rows of `count` results (packed order; `heads` the packed batch's
+ * heads for the node counts; `archive_fitness` NULL for the results'). */
+ce_status ce_dump_rows(const ce_result* results, const uint32_t* heads, const ce_dump_head* dump,
+                       const float* archive_fitness, size_t count, const ce_world* world, uint8_t* rows);
+/* The same on the device (device pointers, `rows` 16-byte aligned),
+ * asynchronous on `stream`; equal to ce_dump_rows to the byte. No
+ * counterpart in the reference, which writes the rows on the host. */
+ce_status ce_dump_rows_device(const ce_result* results, const uint32_t* heads, const ce_dump_head* dump,
+                              const float* archive_fitness, size_t count, const ce_world* world, uint8_t* rows,
+                              void* stream);
+
 /* Shape classes (the niche's aspect axis, from the genes) of a batch packed
  * by ce_pack(pop, indices, n, ..., slots, ...), in packed order. */
 ce_status ce_shape_classes(const ce_population* pop, const uint32_t* indices, size_t n, const uint32_t* slots,
@@ -315,9 +354,14 @@ int ce_free_slots(ce_engine* engine);
 size_t ce_allocated_bytes(ce_engine* engine);
 ce_status ce_release_idle(ce_engine* engine);
 
-/* Records K creatures of `pack` (K = pack->count <= 64): every frame of
- * each trial, frame-major, `stride` float2 slots per creature and frame
- * (src/creature_kernel.rs:312-326); frames = SETTLE + steps + 1. Synchronous. */
+/* Records K creatures of `pack` (K = pack->count <= CE_RECORD_MAX_CREATURES):
+ * every frame of each trial, creature-major then frame-major, `stride`
+ * float2 slots per creature and frame (src/creature_kernel.rs:312-326);
+ * frames = SETTLE + steps + 1 a creature. The reference records one creature
+ * a call; many-creature recordings run as one launch over the GPU. The
+ * frames take K x frames x stride x 8 bytes on the device as well.
+ * Synchronous. */
+#define CE_RECORD_MAX_CREATURES 65536u
 ce_status ce_record(ce_engine* engine, const ce_wave_pack* pack, const ce_world* world,
                     float* frames, size_t frames_cap_floats, ce_result* results);
 

@@ -34,3 +34,20 @@ def test_recorded_frames_decode_to_the_fitness(engine):
         ran = int(round(r["fall_time"] * rate)) if r["fall_time"] > 0 else steps
         com = float((mass * out["positions"][settle + ran, :, 0]).sum() / mass.sum())
         assert abs(com - float(r["fitness"])) <= 1e-3, (c, com, float(r["fitness"]))
+
+
+def test_many_creature_recording_equals_single_recordings(engine):
+    """A recording of 400 creatures runs as one launch over several blocks;
+    each creature's frames and result equal those of recording it alone."""
+    w = WORKLOADS["small"]
+    world = w.world(duration=2.0)
+    wave = ce.pack(ce.generate(w.spec, 400), world)
+    frames, results = engine.record(wave, world)
+    stride = frames.shape[2]
+    for c in (0, 1, 127, 128, 255, 399):
+        one = wave.take([c])
+        f1, r1 = engine.record(one, world)
+        m, n = int(one.heads[0, 1]), int(one.heads[0, 0] & 255)
+        np.testing.assert_array_equal(frames[c][:, :32 + m + n].view(np.uint32), f1[0][:, :32 + m + n].view(np.uint32))
+        np.testing.assert_array_equal(frames[c][:, stride - 1].view(np.uint32), f1[0][:, -1].view(np.uint32))
+        assert results[c:c + 1].view(np.uint32).tolist() == r1.view(np.uint32).tolist()
