@@ -194,6 +194,33 @@ void ground(float x, float amplitude, float tilt, float width, float hurdle, flo
 }
 
 // ------------------------------------------------------------------- model
+// A vector of at most N elements stored inline: the packer's per-creature
+// model holds a few dozen small arrays, and heap allocations for them cost
+// more than the arithmetic. The interface is the part of std::vector used.
+template <class T, size_t N>
+struct Inline {
+    T v[N];
+    size_t n = 0;
+    Inline() = default;
+    explicit Inline(size_t k, const T& x = T()) { assign(k, x); }
+    void assign(size_t k, const T& x) {
+        n = k;
+        for (size_t i = 0; i < k; i++) v[i] = x;
+    }
+    void resize(size_t k) {
+        for (size_t i = n; i < k; i++) v[i] = T();
+        n = k;
+    }
+    void reserve(size_t) {}
+    void push_back(const T& x) { v[n++] = x; }
+    size_t size() const { return n; }
+    T& operator[](size_t i) { return v[i]; }
+    const T& operator[](size_t i) const { return v[i]; }
+    T* data() { return v; }
+    const T* data() const { return v; }
+};
+constexpr size_t kNodesMax = CE_MAX_NODES, kBonesMax = CE_MAX_NODES - 1, kMusclesMax = CE_MAX_MUSCLES;
+
 struct PNode {  // physics::Node, the fields the model reads
     float px, py, radius, friction, mass;
 };
@@ -226,9 +253,9 @@ static float slack_length(const ce_bone_gene* bones, size_t nb, const PNode* nod
 }
 
 // physics::nodes: node masses with bones, organs and muscles.
-static std::vector<PNode> body_nodes(const ce_node_gene* g, size_t n, const ce_bone_gene* bones,
-                                     size_t nb, const ce_muscle_gene* muscles, size_t nm) {
-    std::vector<PNode> nodes(n);
+static Inline<PNode, kNodesMax> body_nodes(const ce_node_gene* g, size_t n, const ce_bone_gene* bones,
+                                           size_t nb, const ce_muscle_gene* muscles, size_t nm) {
+    Inline<PNode, kNodesMax> nodes(n);
     for (size_t i = 0; i < n; i++) {
         nodes[i] = PNode{g[i].x, g[i].y, g[i].diameter * 0.5f, g[i].friction, node_mass(g[i].diameter)};
     }
@@ -271,32 +298,35 @@ struct MuscleModel {
 };
 
 struct Model {
-    std::vector<float> mass, radius, friction;
+    Inline<float, kNodesMax> mass, radius, friction;
     float total_mass = 0, inv_mass = 0;
-    std::vector<uint32_t> pivot;
-    std::vector<int32_t> parent;  // -1 = none
-    std::vector<float> length, lo, hi, rest;
-    std::vector<MuscleModel> muscles;
+    Inline<uint32_t, kBonesMax> pivot;
+    Inline<int32_t, kBonesMax> parent;  // -1 = none
+    Inline<float, kBonesMax> length, lo, hi, rest;
+    Inline<MuscleModel, kMusclesMax> muscles;
     float quake_phase_ = 0, amplitude = 0;
-    std::vector<float> sx, sy;  // gene positions in model order
+    Inline<float, kNodesMax> sx, sy;  // gene positions in model order
 };
 
 // physics2::Model::new (src/physics2.rs:190-350).
 static Model make_model(const ce_node_gene* g, size_t n, const ce_bone_gene* bones, size_t nb,
                         const ce_muscle_gene* mg, size_t nm, uint64_t id, const ce_world& w) {
-    const std::vector<PNode> nodes = body_nodes(g, n, bones, nb, mg, nm);
-    std::vector<uint32_t> order(n);
+    const Inline<PNode, kNodesMax> nodes = body_nodes(g, n, bones, nb, mg, nm);
+    Inline<uint32_t, kNodesMax> order(n);
     order[0] = 0;
     for (size_t j = 0; j < nb; j++) order[j + 1] = bones[j].b;
-    std::vector<uint32_t> record(n, 0);
+    Inline<uint32_t, kNodesMax> record(n, 0);
     for (size_t r = 0; r < n; r++) record[order[r]] = (uint32_t)r;
-    std::vector<int32_t> parent_of_node(n, -1);
+    Inline<int32_t, kNodesMax> parent_of_node(n, -1);
     for (size_t j = 0; j < nb; j++) parent_of_node[bones[j].b] = (int32_t)j;
-    auto angle = [&](size_t j) {
+    // Each bone's direction in the gene pose, once a bone.
+    Inline<float, kBonesMax> angles(nb);
+    for (size_t j = 0; j < nb; j++) {
         const ce_node_gene& p = g[bones[j].a];
         const ce_node_gene& q = g[bones[j].b];
-        return std::atan2(q.y - p.y, q.x - p.x);
-    };
+        angles[j] = std::atan2(q.y - p.y, q.x - p.x);
+    }
+    auto angle = [&](size_t j) { return angles[j]; };
     Model M;
     M.rest.reserve(nb);
     for (size_t j = 0; j < nb; j++) {
@@ -335,7 +365,7 @@ static Model make_model(const ce_node_gene* g, size_t n, const ce_bone_gene* bon
         u.reset = m.reset;
     }
     // Strength from the lighter driven subtree, shared by same-side copies.
-    std::vector<float> subtree(nb);
+    Inline<float, kBonesMax> subtree(nb);
     for (size_t j = 0; j < nb; j++) {
         subtree[j] = nodes[order[j + 1]].mass + (j == 0 ? nodes[order[0]].mass : 0.0f);
     }
@@ -376,7 +406,7 @@ static Model make_model(const ce_node_gene* g, size_t n, const ce_bone_gene* bon
         const float cross = (pa[0] - j[0]) * (pb[1] - j[1]) - (pa[1] - j[1]) * (pb[0] - j[0]);
         return Key{std::min(m.bone_a, m.bone_b), std::max(m.bone_a, m.bone_b), cross >= 0.0f};
     };
-    std::vector<Key> groups(nm);
+    Inline<Key, kMusclesMax> groups(nm);
     for (size_t k = 0; k < nm; k++) groups[k] = group(mg[k]);
     for (size_t k = 0; k < nm; k++) {
         MuscleModel& u = M.muscles[k];
@@ -418,7 +448,8 @@ static Model make_model(const ce_node_gene* g, size_t n, const ce_bone_gene* bon
 
 struct State {
     float x0[2], v0[2], th0, w0;
-    std::vector<float> q, qd, th, om, px, py, vx, vy;
+    Inline<float, kBonesMax> q, qd, th, om;
+    Inline<float, kNodesMax> px, py, vx, vy;
 };
 
 // physics2::Model::kinematics (src/physics2.rs:402-418).
@@ -1033,7 +1064,7 @@ extern "C" ce_status ce_gene_gradients(const ce_population* pop, const uint32_t*
         const float* rec = grads + c * per;
         const size_t n = gm.node_count, nb = gm.bone_count, nm = gm.muscle_count;
         // d J / d (gene node mass): the kernel's rows, then the strengths.
-        const std::vector<PNode> body = body_nodes(ng, n, bg, nb, mg, nm);
+        const Inline<PNode, kNodesMax> body = body_nodes(ng, n, bg, nb, mg, nm);
         std::vector<uint32_t> row_of(n, 0);
         row_of[0] = 0;
         for (size_t j = 0; j < nb; j++) row_of[bg[j].b] = (uint32_t)(j + 1);
