@@ -32,7 +32,7 @@ import time
 
 import numpy as np
 
-from . import api
+from . import api, shard
 
 MAX_BONE = 2.0            # physics::Limits::DEFAULT.max_bone (src/physics.rs:142-153)
 MAX_STROKE = 2.0          # .max_stroke
@@ -42,6 +42,7 @@ DIAMETER = (0.06, 0.12)   # the workloads' node diameters
 FRICTION = (0.0, 1.0)     # the workloads' node friction
 STRENGTH = (0.5, 1.5)     # the workloads' strength factors
 UNIT = dict(length=0.02, phase=0.05, duty=0.05, friction=0.03, strength=0.05)
+SAMPLE_BLOCK = 4096       # samples drawn from one random stream
 
 
 def take(pop: api.Population, idx, ids=None) -> api.Population:
@@ -87,18 +88,27 @@ def _size(pop: api.Population) -> np.ndarray:
     return np.clip(size, 0.05, 10.0).astype(np.float32)
 
 
-def samples(parents: api.Population, count: int, sigma: float, seed: int, first_id: int = 1):
-    """`count` samples, sample i a child of parent i mod len(parents) with
-    every parameter-vector coordinate moved by sigma x N(0, 1) (seeded), ids
-    first_id + i. Returns (population, parent of each sample)."""
-    parent = np.arange(count, dtype=np.int64) % len(parents)
-    pop = take(parents, parent, first_id + np.arange(count, dtype=np.uint64))
-    rng = np.random.default_rng(seed)
+def concat(pops) -> api.Population:
+    """Populations one after another as one population."""
+    pops = list(pops)
+    genomes = np.concatenate([p.genomes for p in pops])
+    for field, rows in (("node_start", "nodes"), ("bone_start", "bones"), ("muscle_start", "muscles")):
+        offsets = np.cumsum([0] + [len(getattr(p, rows)) for p in pops[:-1]])
+        genomes[field] += np.repeat(offsets, [len(p.genomes) for p in pops]).astype(np.uint32)
+    strength = None if pops[0].strength is None else np.concatenate([p.strength for p in pops])
+    return api.Population(np.concatenate([p.nodes for p in pops]), np.concatenate([p.bones for p in pops]),
+                          np.concatenate([p.muscles for p in pops]), genomes, strength)
+
+
+def _perturb(pop: api.Population, sigma: float, rng) -> None:
+    """Every parameter-vector coordinate of every creature of `pop` moved by
+    sigma x N(0, 1), back to genes with the clamps (in place)."""
     f32 = np.float32
 
     def noise(n):
         return f32(sigma) * rng.standard_normal(n, dtype=f32)
 
+    count = len(pop)
     n = pop.nodes
     n["x"] += noise(len(n))
     n["y"] = np.maximum(n["y"] + noise(len(n)), f32(0.0))
@@ -128,7 +138,27 @@ def samples(parents: api.Population, count: int, sigma: float, seed: int, first_
     m["stiffness"] = np.clip(np.exp(np.log(np.maximum(m["stiffness"], f32(1e-3))) + noise(len(m))), f32(1.0),
                              f32(120.0))
     m["reset"] = np.mod(m["reset"] + noise(len(m)), f32(1.0))
-    return pop, parent
+
+
+def samples(parents: api.Population, count: int, sigma: float, seed: int, first_id: int = 1, first: int = 0):
+    """Samples [first, first + count): sample i is a child of parent
+    i mod len(parents) with every parameter-vector coordinate moved by
+    sigma x N(0, 1) and id first_id + i. Its moves come from the random
+    stream of its block of SAMPLE_BLOCK samples, seeded with (seed, block),
+    so a sample is the same whichever range of samples a rank draws.
+    Returns (population, parent of each sample)."""
+    P = len(parents)
+    parts = []
+    blocks = range(first // SAMPLE_BLOCK, (first + count - 1) // SAMPLE_BLOCK + 1) if count > 0 else range(0)
+    for blk in blocks:
+        c0, c1 = blk * SAMPLE_BLOCK, (blk + 1) * SAMPLE_BLOCK
+        idx = np.arange(c0, c1, dtype=np.int64)
+        pop = take(parents, idx % P, first_id + idx.astype(np.uint64))
+        _perturb(pop, sigma, np.random.default_rng([seed, blk]))
+        lo, hi = max(first, c0) - c0, min(first + count, c1) - c0
+        parts.append(pop if (lo, hi) == (0, SAMPLE_BLOCK) else take(pop, np.arange(lo, hi)))
+    pop = concat(parts) if parts else take(parents, np.zeros(0, np.int64))
+    return pop, np.arange(first, first + count, dtype=np.int64) % P
 
 
 def ascend(pop: api.Population, muscle_grads: np.ndarray, node_grads: np.ndarray, step: float) -> api.Population:
@@ -180,7 +210,7 @@ def _evaluate(engine, pop, world, chunk: int):
 
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
-           resample: bool = True) -> dict:
+           resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None) -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -190,26 +220,36 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
        same elites children (σ = sigma) for about the same GPU time, each
        elite keeping the best of itself and its children. Fitness gained is
        the elites' mean best fitness minus their mean sampled fitness; GPU
-       seconds are the kernels' device time (host packing not included)."""
-    report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step)
+       seconds are the kernels' device time summed over ranks (host packing
+       not included).
+
+    Over several ranks (one GPU each, `group` a torch.distributed group):
+    rank r draws and evaluates samples [count r / W, count (r + 1) / W), the
+    elites are chosen once over all ranks (an all-gather of each rank's best
+    (fitness, sample) pairs), and each rank refines and resamples the elites
+    among its own samples; the report's figures are totals over the ranks,
+    the same on every rank."""
+    report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
+                  ranks=world_size)
+    lo, hi = count * rank // world_size, count * (rank + 1) // world_size
     t0 = time.perf_counter()
     base = api.generate(spec, parents)
-    pop, _ = samples(base, count, sigma, seed)
+    pop, _ = samples(base, hi - lo, sigma, seed, first=lo)
     report["host_sample_s"] = time.perf_counter() - t0
     fit, busy = _evaluate(engine, pop, world, chunk)
-    report["sample_gpu_s"] = busy
-    order = np.argsort(-np.where(np.isfinite(fit) & (fit > -1e19), fit, -np.inf), kind="stable")
-    top = order[:elites]
-    elite = take(pop, top)
-    f0 = fit[top].astype(np.float64)
-    report["elite_mean_fitness"] = float(f0.mean())
-    # Gradient refinement.
+    valid = np.isfinite(fit) & (fit > -1e19)
+    _, chosen = shard.global_top_k(np.where(valid, fit, -np.inf), lo + np.arange(hi - lo), elites, world_size, group,
+                                   device)
+    mine = np.sort(chosen[(chosen >= lo) & (chosen < hi)]) - lo
+    elite = take(pop, mine)
+    f0 = fit[mine].astype(np.float64)
+    # Gradient refinement of this rank's elites.
     best = f0.copy()
     x = elite
     refine_s = 0.0
+    first_equal = True
     t0 = time.perf_counter()
-    first_equal = None
-    for k in range(steps):
+    for k in range(steps if len(mine) else 0):
         wave = api.pack(x, world)
         with engine.forward(wave, world) as tape:
             fk = _fitness(wave, tape.results).astype(np.float64)
@@ -223,28 +263,37 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
         mg, ng = api.gene_gradients(x, wave, world, g, shape)
         x = ascend(x, mg, ng, step)
-    fk, secs = _evaluate(engine, x, world, chunk)
-    refine_s += secs
-    best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
-    gain = float((best - f0).mean())
-    report["refine"] = dict(first_equal=first_equal, gpu_s=refine_s, mean_best=float(best.mean()), gain=gain, gain_per_gpu_s=gain / refine_s,
-                            improved=float((best > f0).mean()), host_s=time.perf_counter() - t0)
+    if len(mine):
+        fk, secs = _evaluate(engine, x, world, chunk)
+        refine_s += secs
+        best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+    host_refine = time.perf_counter() - t0
+    tot = shard.all_sum([len(mine), f0.sum(), best.sum(), (best > f0).sum(), busy, refine_s,
+                         0.0 if first_equal else 1.0], world_size, group, device)
+    n_el = max(tot[0], 1.0)
+    report["sample_gpu_s"] = tot[4]
+    report["elite_mean_fitness"] = tot[1] / n_el
+    gain = (tot[2] - tot[1]) / n_el
+    report["refine"] = dict(first_equal=tot[6] == 0.0, gpu_s=tot[5], mean_best=tot[2] / n_el, gain=gain,
+                            gain_per_gpu_s=gain / tot[5], improved=tot[3] / n_el, host_s=host_refine)
     if resample:
-        per = max(1, int(round(refine_s / (report["sample_gpu_s"] / count) / elites)))
+        per = max(1, int(round(tot[5] / (tot[4] / count) / elites)))
         t0 = time.perf_counter()
         bestr = f0.copy()
         secs = 0.0
-        rounds = max(1, chunk // elites)
-        for r0 in range(0, per, rounds):
-            n = min(rounds, per - r0) * elites
-            kids, parent = samples(elite, n, sigma, seed + 1 + r0)
+        rounds = max(1, chunk // max(len(mine), 1))
+        for r0 in range(0, per if len(mine) else 0, rounds):
+            n = min(rounds, per - r0) * len(mine)
+            # A stream of its own for every rank and chunk.
+            kids, parent = samples(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + r0 // rounds)
             # Children keep their elite's id, so they see its tremor phase.
             kids.genomes["id"] = elite.genomes["id"][parent]
-            fk, busy = _evaluate(engine, kids, world, chunk)
-            secs += busy
+            fk, busy_r = _evaluate(engine, kids, world, chunk)
+            secs += busy_r
             np.maximum.at(bestr, parent, np.where(fk > -1e19, fk, -np.inf).astype(np.float64))
-        gain_r = float((bestr - f0).mean())
-        report["resample"] = dict(children_per_elite=per, gpu_s=secs, mean_best=float(bestr.mean()), gain=gain_r,
-                                  gain_per_gpu_s=gain_r / secs, improved=float((bestr > f0).mean()),
+        tr = shard.all_sum([bestr.sum(), (bestr > f0).sum(), secs], world_size, group, device)
+        gain_r = (tr[0] - tot[1]) / n_el
+        report["resample"] = dict(children_per_elite=per, gpu_s=tr[2], mean_best=tr[0] / n_el, gain=gain_r,
+                                  gain_per_gpu_s=gain_r / tr[2], improved=tr[1] / n_el,
                                   host_s=time.perf_counter() - t0)
     return report

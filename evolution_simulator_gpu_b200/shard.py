@@ -63,3 +63,47 @@ def evaluate_sharded(evaluate: Callable[[WavePack], np.ndarray], wave: WavePack,
         k = int(b[r + 1] - b[r])
         out[b[r]:b[r + 1]] = parts[r].cpu().numpy()[:k].reshape(-1).view(RESULT_DTYPE)
     return out
+
+
+def global_top_k(values: np.ndarray, ids: np.ndarray, k: int, world_size: int = 1, group=None, device=None):
+    """The k largest `values` over all ranks with their `ids` (ties: the
+    smaller id first), the same on every rank: each rank's own top k, an
+    all-gather of k (value, id) pairs a rank, and one selection. Values that
+    are not finite rank last."""
+    v = np.where(np.isfinite(values), np.asarray(values, np.float64), -np.inf)
+    ids = np.asarray(ids, np.int64)
+    order = np.lexsort((ids, -v))[:k]
+    v, ids = v[order], ids[order]
+    if world_size == 1:
+        return v, ids
+    import torch
+    import torch.distributed as dist
+    pad = k - len(v)
+    v = np.concatenate([v, np.full(pad, -np.inf)])
+    ids = np.concatenate([ids, np.full(pad, np.iinfo(np.int64).max, np.int64)])
+    tv, ti = torch.from_numpy(v), torch.from_numpy(ids)
+    if device is not None:
+        tv, ti = tv.to(device), ti.to(device)
+    pv = [torch.empty_like(tv) for _ in range(world_size)]
+    pi = [torch.empty_like(ti) for _ in range(world_size)]
+    dist.all_gather(pv, tv, group=group)
+    dist.all_gather(pi, ti, group=group)
+    v = np.concatenate([p.cpu().numpy() for p in pv])
+    ids = np.concatenate([p.cpu().numpy() for p in pi])
+    order = np.lexsort((ids, -v))[:k]
+    keep = ids[order] != np.iinfo(np.int64).max
+    return v[order][keep], ids[order][keep]
+
+
+def all_sum(values, world_size: int = 1, group=None, device=None) -> np.ndarray:
+    """Element-wise sum of a few float64 values over the ranks."""
+    x = np.asarray(values, np.float64)
+    if world_size == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(x.copy())
+    if device is not None:
+        t = t.to(device)
+    dist.all_reduce(t, group=group)
+    return t.cpu().numpy()
