@@ -162,6 +162,38 @@ ce_status check_world(const ce_world* w) {
     return CE_OK;
 }
 
+// Copies `n` bytes from pageable `src` to pinned `dst` on several host
+// threads (one thread copies a few GB/s; a generation's records are GBs).
+void parallel_copy(char* dst, const char* src, size_t n) {
+    const unsigned threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (threads == 1 || n < ((size_t)8 << 20)) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    const size_t per = ((n + threads - 1) / threads + 4095) & ~(size_t)4095;
+    std::vector<std::thread> pool;
+    for (size_t at = per; at < n; at += per) {
+        pool.emplace_back([=] { std::memcpy(dst + at, src + at, std::min(per, n - at)); });
+    }
+    std::memcpy(dst, src, std::min(per, n));
+    for (std::thread& t : pool) t.join();
+}
+
+// Stages `n` bytes of `src` in the pinned `staging` buffer and copies them to
+// `dev` on `stream`, 256 MB at a time, so that the copy of one chunk to the
+// GPU runs while the next chunk is staged.
+cudaError_t staged_upload(void* dev, char* staging, const void* src, size_t n, cudaStream_t stream) {
+    const size_t chunk = (size_t)256 << 20;
+    for (size_t at = 0; at < n; at += chunk) {
+        const size_t len = std::min(chunk, n - at);
+        parallel_copy(staging + at, static_cast<const char*>(src) + at, len);
+        const cudaError_t e =
+            cudaMemcpyAsync(static_cast<char*>(dev) + at, staging + at, len, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Splits the packed batch into size classes by node count (bodies of at most
 // kSmallBody nodes, and larger ones). Each class runs as one launch whose
 // claim queues are its node counts (kernels.h); the bucketing kernels build
@@ -377,16 +409,12 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
         (s = sl.h_results.ensure(res_b))) {
         return s;
     }
-    // Stage the batch in pinned memory, then copy it up asynchronously.
+    // Stage the batch in pinned memory and copy it up, chunk by chunk.
     char* up = static_cast<char*>(sl.h_upload.ptr);
-    std::memcpy(up, pack->lanes, lanes_b);
-    std::memcpy(up + lanes_b, pack->muscles, mus_b);
-    std::memcpy(up + lanes_b + mus_b, pack->heads, heads_b);
     cudaStream_t st = sl.stream;
-    CE_TRY(cudaMemcpyAsync(sl.d_lanes.ptr, up, lanes_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-    CE_TRY(cudaMemcpyAsync(sl.d_muscles.ptr, up + lanes_b, mus_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-    CE_TRY(cudaMemcpyAsync(sl.d_heads.ptr, up + lanes_b + mus_b, heads_b, cudaMemcpyHostToDevice, st),
-           "cudaMemcpyAsync");
+    CE_TRY(staged_upload(sl.d_lanes.ptr, up, pack->lanes, lanes_b, st), "cudaMemcpyAsync");
+    CE_TRY(staged_upload(sl.d_muscles.ptr, up + lanes_b, pack->muscles, mus_b, st), "cudaMemcpyAsync");
+    CE_TRY(staged_upload(sl.d_heads.ptr, up + lanes_b + mus_b, pack->heads, heads_b, st), "cudaMemcpyAsync");
     CE_TRY(cudaEventRecord(sl.start, st), "cudaEventRecord");
     const cek::Buckets bk = cek::bucket_layout(sl.d_buckets.ptr, pack->count);
     CE_TRY(cek::launch_bucket(static_cast<const uint4*>(sl.d_heads.ptr), 0u, (uint32_t)pack->count, bk, st),
@@ -476,7 +504,10 @@ extern "C" ce_status ce_poll(ce_engine* e, int64_t timeout_us, uint64_t* ticket,
     }
     float ms = 0.0f;
     CE_TRY(cudaEventElapsedTime(&ms, sl.start, sl.stop), "cudaEventElapsedTime");
-    if (out) std::memcpy(out, sl.h_results.ptr, sl.count * sizeof(ce_result));
+    if (out) {
+        parallel_copy(reinterpret_cast<char*>(out), static_cast<const char*>(sl.h_results.ptr),
+                      sl.count * sizeof(ce_result));
+    }
     *ticket = sl.ticket;
     *n = sl.count;
     if (busy_seconds) *busy_seconds = ms * 1e-3;
