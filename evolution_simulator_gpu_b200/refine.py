@@ -263,21 +263,25 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
         mg, ng = api.gene_gradients(x, wave, world, g, shape)
         x = ascend(x, mg, ng, step)
+    last_s = 0.0
     if len(mine):
-        fk, secs = _evaluate(engine, x, world, chunk)
-        refine_s += secs
+        fk, last_s = _evaluate(engine, x, world, chunk)
+        refine_s += last_s
         best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
     host_refine = time.perf_counter() - t0
     tot = shard.all_sum([len(mine), f0.sum(), best.sum(), (best > f0).sum(), busy, refine_s,
-                         0.0 if first_equal else 1.0], world_size, group, device)
+                         0.0 if first_equal else 1.0, last_s], world_size, group, device)
     n_el = max(tot[0], 1.0)
     report["sample_gpu_s"] = tot[4]
     report["elite_mean_fitness"] = tot[1] / n_el
     gain = (tot[2] - tot[1]) / n_el
-    report["refine"] = dict(first_equal=tot[6] == 0.0, gpu_s=tot[5], mean_best=tot[2] / n_el, gain=gain,
+    report["refine"] = dict(first_equal=bool(tot[6] == 0.0), gpu_s=float(tot[5]), mean_best=tot[2] / n_el, gain=gain,
                             gain_per_gpu_s=gain / tot[5], improved=tot[3] / n_el, host_s=host_refine)
     if resample:
-        per = max(1, int(round(tot[5] / (tot[4] / count) / elites)))
+        # Children per elite for about the refinement's GPU time, from the
+        # time the elites' own last evaluation took a trial.
+        per_trial = tot[7] / n_el if tot[7] > 0 else tot[4] / count
+        per = max(1, int(round(tot[5] / per_trial / n_el)))
         t0 = time.perf_counter()
         bestr = f0.copy()
         secs = 0.0
