@@ -278,26 +278,26 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     report["refine"] = dict(first_equal=bool(tot[6] == 0.0), gpu_s=float(tot[5]), mean_best=tot[2] / n_el, gain=gain,
                             gain_per_gpu_s=gain / tot[5], improved=tot[3] / n_el, host_s=host_refine)
     if resample:
-        # Children per elite for about the refinement's GPU time, from the
-        # time the elites' own last evaluation took a trial.
-        per_trial = tot[7] / n_el if tot[7] > 0 else tot[4] / count
-        per = max(1, int(round(tot[5] / per_trial / n_el)))
+        # Rounds of children (one child per elite a round, `rounds` rounds a
+        # batch) until this rank has spent its refinement's GPU time.
         t0 = time.perf_counter()
         bestr = f0.copy()
         secs = 0.0
-        rounds = max(1, chunk // max(len(mine), 1))
-        for r0 in range(0, per if len(mine) else 0, rounds):
-            n = min(rounds, per - r0) * len(mine)
-            # A stream of its own for every rank and chunk.
-            kids, parent = samples(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + r0 // rounds)
+        per = 0
+        rounds = max(1, min(chunk, 1 << 19) // max(len(mine), 1))
+        while len(mine) and secs < refine_s:
+            n = rounds * len(mine)
+            # A stream of its own for every rank and batch.
+            kids, parent = samples(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + per // rounds)
             # Children keep their elite's id, so they see its tremor phase.
             kids.genomes["id"] = elite.genomes["id"][parent]
             fk, busy_r = _evaluate(engine, kids, world, chunk)
             secs += busy_r
+            per += rounds
             np.maximum.at(bestr, parent, np.where(fk > -1e19, fk, -np.inf).astype(np.float64))
-        tr = shard.all_sum([bestr.sum(), (bestr > f0).sum(), secs], world_size, group, device)
+        tr = shard.all_sum([bestr.sum(), (bestr > f0).sum(), secs, per], world_size, group, device)
         gain_r = (tr[0] - tot[1]) / n_el
-        report["resample"] = dict(children_per_elite=per, gpu_s=tr[2], mean_best=tr[0] / n_el, gain=gain_r,
+        report["resample"] = dict(children_per_elite=tr[3] / world_size, gpu_s=tr[2], mean_best=tr[0] / n_el, gain=gain_r,
                                   gain_per_gpu_s=gain_r / tr[2], improved=tr[1] / n_el,
                                   host_s=time.perf_counter() - t0)
     return report
