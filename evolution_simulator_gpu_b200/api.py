@@ -189,6 +189,10 @@ def _bind(lib: C.CDLL) -> None:
         "ce_metrics_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_shape_classes": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_void_p]),
+        "ce_sample_rows": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_size_t, P(C.c_size_t), P(C.c_size_t),
+                                     P(C.c_size_t)]),
+        "ce_sample_device": (C.c_int, [P(PopulationC), C.c_uint64, C.c_size_t, C.c_float, C.c_uint64, C.c_uint64,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_dump_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_dump_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World),
                                           C.c_void_p, C.c_void_p]),
@@ -229,7 +233,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
-            "ce_replay_decode", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
+            "ce_replay_decode", "ce_sample_rows", "ce_sample_device", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
             "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
 
 

@@ -31,7 +31,8 @@ NVCC_FLAGS = [
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp"]
 
-CUDA_SOURCES = ["advance.cu", "adjoint.cu", "bucket.cu", "engine.cu", "metrics.cu", "peak.cu", "noalloc.cu"]
+CUDA_SOURCES = ["advance.cu", "adjoint.cu", "bucket.cu", "engine.cu", "metrics.cu", "peak.cu", "noalloc.cu",
+                "sample.cu"]
 CXX_SOURCES = ["host_model.cpp", "generator.cpp"]
 
 

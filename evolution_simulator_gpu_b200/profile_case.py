@@ -60,6 +60,7 @@ def main() -> None:
     ap.add_argument("--parents", type=int, default=1024)
     ap.add_argument("--elites", type=int, default=16_384)
     ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--sampler", default="device", choices=["device", "host"], help="where the samples are drawn")
     args = ap.parse_args()
     if args.generations:
         return generations(args)
@@ -72,7 +73,7 @@ def main() -> None:
         w = WORKLOADS[args.workload]
         with ce.Engine(0) as eng:
             out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
-                                count=args.creatures, elites=args.elites, steps=args.steps)
+                                count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler)
         out.update(workload=args.workload, seconds=args.seconds)
         print(json.dumps(out))
         return

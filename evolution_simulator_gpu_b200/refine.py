@@ -161,6 +161,49 @@ def samples(parents: api.Population, count: int, sigma: float, seed: int, first_
     return pop, np.arange(first, first + count, dtype=np.int64) % P
 
 
+def samples_gpu(parents: api.Population, count: int, sigma: float, seed: int, first_id: int = 1, first: int = 0,
+                device: int = 0):
+    """Samples [first, first + count) drawn on the GPU (ce_sample_device):
+    the moves of `samples`, from a counter-based hash of (seed, sample, gene,
+    field) instead of numpy's streams. Returns (population on the host,
+    parent of each sample)."""
+    import torch
+    import ctypes as C
+    dev = torch.device("cuda", device)
+    par = take(parents, np.arange(len(parents)))  # genes packed in order from row 0
+
+    def up(arr):
+        return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(dev)
+
+    dn, db, dm, dg = up(par.nodes), up(par.bones), up(par.muscles), up(par.genomes)
+    ds = None if par.strength is None else up(par.strength)
+    rn, rb, rm = C.c_size_t(), C.c_size_t(), C.c_size_t()
+    L = api.lib()
+    api._check(L.ce_sample_rows(api._ptr(par.genomes), len(par), first, count, C.byref(rn), C.byref(rb), C.byref(rm)),
+               "ce_sample_rows")
+
+    def out(rows, dtype):
+        return torch.empty(max(rows * dtype.itemsize, 1), dtype=torch.uint8, device=dev)
+
+    on, ob, om = out(rn.value, api.NODE_DTYPE), out(rb.value, api.BONE_DTYPE), out(rm.value, api.MUSCLE_DTYPE)
+    og, ost = out(count, api.GENOME_DTYPE), out(rm.value, np.dtype(np.float32))
+    pc = api.PopulationC(dn.data_ptr(), db.data_ptr(), dm.data_ptr(), dg.data_ptr(), len(par),
+                         None if ds is None else ds.data_ptr())
+    stream = torch.cuda.current_stream(dev)
+    api._check(L.ce_sample_device(C.byref(pc), first, count, sigma, seed, first_id, on.data_ptr(), ob.data_ptr(),
+                                  om.data_ptr(), ost.data_ptr(), og.data_ptr(), stream.cuda_stream),
+               "ce_sample_device")
+    stream.synchronize()
+
+    def back(t, rows, dtype):
+        return t.cpu().numpy()[:rows * dtype.itemsize].view(dtype).copy()
+
+    pop = api.Population(back(on, rn.value, api.NODE_DTYPE), back(ob, rb.value, api.BONE_DTYPE),
+                         back(om, rm.value, api.MUSCLE_DTYPE), back(og, count, api.GENOME_DTYPE),
+                         None if ds is None else back(ost, rm.value, np.dtype(np.float32)))
+    return pop, np.arange(first, first + count, dtype=np.int64) % len(parents)
+
+
 def ascend(pop: api.Population, muscle_grads: np.ndarray, node_grads: np.ndarray, step: float) -> api.Population:
     """One clipped gradient-ascent step on the differentiated coordinates
     (see the module docstring), from gene gradients (gene_gradients: per
@@ -210,7 +253,8 @@ def _evaluate(engine, pop, world, chunk: int):
 
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
-           resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None) -> dict:
+           resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None,
+           sampler: str = "host") -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -228,13 +272,15 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     elites are chosen once over all ranks (an all-gather of each rank's best
     (fitness, sample) pairs), and each rank refines and resamples the elites
     among its own samples; the report's figures are totals over the ranks,
-    the same on every rank."""
+    the same on every rank. `sampler` "device" draws the samples on the GPU
+    (samples_gpu), "host" with numpy (samples)."""
+    draw = samples if sampler == "host" else samples_gpu
     report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
-                  ranks=world_size)
+                  ranks=world_size, sampler=sampler)
     lo, hi = count * rank // world_size, count * (rank + 1) // world_size
     t0 = time.perf_counter()
     base = api.generate(spec, parents)
-    pop, _ = samples(base, hi - lo, sigma, seed, first=lo)
+    pop, _ = draw(base, hi - lo, sigma, seed, first=lo)
     report["host_sample_s"] = time.perf_counter() - t0
     fit, busy = _evaluate(engine, pop, world, chunk)
     valid = np.isfinite(fit) & (fit > -1e19)
@@ -288,7 +334,7 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         while len(mine) and secs < refine_s:
             n = rounds * len(mine)
             # A stream of its own for every rank and batch.
-            kids, parent = samples(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + per // rounds)
+            kids, parent = draw(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + per // rounds)
             # Children keep their elite's id, so they see its tremor phase.
             kids.genomes["id"] = elite.genomes["id"][parent]
             fk, busy_r = _evaluate(engine, kids, world, chunk)

@@ -294,6 +294,25 @@ ce_status ce_dump_rows_device(const ce_result* results, const uint32_t* heads, c
                               const float* archive_fitness, size_t count, const ce_world* world, uint8_t* rows,
                               void* stream);
 
+/* ---- samples of parent genomes (the refined search's ask step) ---- */
+/* Sample g is a child of parent g mod P with every coordinate of the
+ * optimizer's parameter vector of its body (src/qd.rs:2700-2770) moved by
+ * sigma x N(0, 1) and put back with apply_parameters' clamps
+ * (src/qd.rs:2773-2811), diameter and friction held to the workloads'
+ * ranges; its id is first_id + g, its strength factors its parent's. The
+ * deviates come from a counter-based hash of (seed, g, gene, field), so a
+ * sample does not depend on the range a call draws. No counterpart in the
+ * reference, which samples on the host. ce_sample_rows gives the rows of
+ * samples [first, first + count) from the parents' (host) genomes;
+ * ce_sample_device writes them (device pointers; the parents' genes packed
+ * in order from row 0; `strength` may be NULL), asynchronous on `stream`
+ * after a small synchronous read of the parents' genomes. */
+ce_status ce_sample_rows(const ce_genome* parent_genomes, size_t parents, uint64_t first, size_t count,
+                         size_t* nodes, size_t* bones, size_t* muscles);
+ce_status ce_sample_device(const ce_population* parents, uint64_t first, size_t count, float sigma, uint64_t seed,
+                           uint64_t first_id, ce_node_gene* nodes, ce_bone_gene* bones, ce_muscle_gene* muscles,
+                           float* strength, ce_genome* genomes, void* stream);
+
 /* Shape classes (the niche's aspect axis, from the genes) of a batch packed
  * by ce_pack(pop, indices, n, ..., slots, ...), in packed order. */
 ce_status ce_shape_classes(const ce_population* pop, const uint32_t* indices, size_t n, const uint32_t* slots,
