@@ -99,3 +99,50 @@ def test_recording_matches_reference_frames(engine):
         np.testing.assert_array_equal(mine[:, :32 + m + n].view(np.uint32), rf[:, :32 + m + n].view(np.uint32))
         np.testing.assert_array_equal(mine[:, stride - 1].view(np.uint32), rf[:, s1 - 1].view(np.uint32))
         assert bits(res[c:c + 1]).tolist() == bits(rr).tolist()
+
+
+@pytest.mark.parametrize("effects", [False, True])
+def test_largest_bodies_match_bits(engine, effects):
+    """Bodies at the engine's limits: 28-32 nodes and 64-96 muscles, all of
+    them one size class, the widest tables and lane slots."""
+    spec = ce.GenSpecPy(seed=9, min_nodes=28, max_nodes=32, muscle_rule=1, min_muscles=64, max_muscles=96,
+                        joint_lo_deg=30.0, joint_hi_deg=150.0)
+    world = ce.make_world(**effects_world_kw()) if effects else ce.make_world()
+    res = compare(engine, spec, world, 384, duration=3.0)
+    assert (res["fitness"] > -1e19).any()
+
+
+def _two_node_population(n):
+    rng = np.random.default_rng(4)
+    nodes = np.zeros(2 * n, ce.api.NODE_DTYPE)
+    nodes["x"] = rng.uniform(0, 1, 2 * n)
+    nodes["y"] = rng.uniform(0, 1, 2 * n)
+    nodes["diameter"] = rng.uniform(0.06, 0.12, 2 * n)
+    nodes["friction"] = rng.uniform(0, 1, 2 * n)
+    bones = np.zeros(n, ce.api.BONE_DTYPE)
+    bones["a"], bones["b"] = 0, 1
+    d = np.hypot(nodes["x"][1::2] - nodes["x"][0::2], nodes["y"][1::2] - nodes["y"][0::2])
+    bones["rest_length"] = np.clip(d, 0.03, 2.0)
+    bones["min_angle"], bones["max_angle"] = -1.0, 1.0
+    genomes = np.zeros(n, ce.api.GENOME_DTYPE)
+    genomes["node_start"] = 2 * np.arange(n)
+    genomes["node_count"] = 2
+    genomes["bone_start"] = np.arange(n)
+    genomes["bone_count"] = 1
+    genomes["id"] = 1 + np.arange(n)
+    return ce.Population(nodes, bones, np.zeros(0, ce.api.MUSCLE_DTYPE), genomes, np.zeros(0, np.float32))
+
+
+def test_two_node_bodies_and_one_creature_batches_match_bits(engine):
+    """The smallest body (two nodes, one bone, no joint, no muscle) in the
+    calm and the effects world, in a batch and as a batch of one."""
+    pop = _two_node_population(200)
+    for world in (ce.make_world(duration=3.0), ce.make_world(duration=3.0, **effects_world_kw())):
+        wave = ce.pack(pop, world)
+        mine, _ = engine.run(wave, world)
+        ref, _ = RefKernel(ce.world_flags(world)).run(wave, ce.make_params(world))
+        assert (bits(mine) == bits(ref)).all()
+        for c in (0, 57, 199):
+            one = wave.take([c])
+            m1, _ = engine.run(one, world)
+            assert (bits(m1) == bits(mine[c:c + 1])).all()
