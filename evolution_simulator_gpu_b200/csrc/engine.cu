@@ -111,6 +111,7 @@ struct ce_engine {
     int sms = 0;
     unsigned ctas_per_sm = 0;  // 0: from the occupancy of each kernel
     unsigned chunk_k = 4;
+    size_t smem_optin = 0;  // shared memory a block may use
     unsigned small_body = kSmallBody;
     std::vector<Slot> slots;
     std::deque<size_t> pending;  // slot indices, oldest first
@@ -253,6 +254,7 @@ extern "C" ce_status ce_open(int device, const ce_options* options, ce_engine** 
     ce_engine* e = new ce_engine();
     e->device = device;
     e->sms = prop.multiProcessorCount;
+    e->smem_optin = prop.sharedMemPerBlockOptin;
     unsigned nslots = 4;
     if (options) {
         if (options->slots) nslots = options->slots;
@@ -732,6 +734,14 @@ extern "C" ce_status ce_forward(ce_engine* e, const ce_wave_pack* pack, const ce
         t->mm = std::max(t->mm, c.mm);
     }
     t->rate = (int)ce::world_rate(*w);
+    if (cek::adjoint_smem_bytes(t->rows, t->mm, cek::kBlock) > e->smem_optin) {
+        const std::string why = "ce_forward: bodies of " + std::to_string(t->rows) + " nodes and " +
+                                std::to_string(t->mm) + " muscles need more shared memory for the backward pass "
+                                "than a block has";
+        ce_tape_free(t);
+        set_error(why);
+        return CE_ERR_UNSUPPORTED;
+    }
     ce_make_params(w, 0, (uint32_t)pack->count, 0, &t->params);
     t->ckpts = (t->params.steps + 15u) / 16u;
     auto fail = [&](ce_status st) {

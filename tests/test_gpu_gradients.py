@@ -214,3 +214,9 @@ def test_gradients_refuse_unsupported_batches(engine):
     assert err.value.status == ce.CE_ERR_UNSUPPORTED
     with pytest.raises(ce.EngineError):
         engine.forward(wave, world, checkpoint_every=128)
+    # Bodies whose backward tables do not fit a block's shared memory.
+    big = ce.GenSpecPy(seed=9, min_nodes=32, max_nodes=32, muscle_rule=1, min_muscles=96, max_muscles=96)
+    wave = ce.pack(ce.generate(big, 8), world)
+    with pytest.raises(ce.EngineError) as err:
+        engine.forward(wave, world)
+    assert err.value.status == ce.CE_ERR_UNSUPPORTED
