@@ -72,7 +72,6 @@ __device__ __forceinline__ float ice_slope(float x) {
 struct AdjointLayout {
     unsigned grad;    // 3 a muscle: (amp, hill, cap, 1/capacity), (phase, duty, 1/duty, 1/(1-duty)), (stiffness)
     unsigned fric;    // friction gradient, 4 nodes a line
-    unsigned mass;    // mass gradient, 4 nodes a line
     unsigned force;   // muscle force on each node in the substep, 2 nodes a line
     unsigned drag;    // bone j: the velocities of its ends before its drag
     unsigned bones;   // bone j: the positions of its ends before its projection
@@ -86,8 +85,6 @@ struct AdjointLayout {
         A.grad = at;
         at += 3u * mm;
         A.fric = at;
-        at += (rows + 3u) / 4u;
-        A.mass = at;
         at += (rows + 3u) / 4u;
         A.force = at;
         at += (rows + 1u) / 2u;
@@ -136,6 +133,7 @@ struct Backward {
     using T = Trial<W, false, RATE>;
     const Body& b;
     const NodeTables& g;  // adjoints: positions, velocities, start positions / forces, (energy, demand)
+    float* gmass;         // d J / d mass of node i at gmass[i * g.stride] (shared memory)
     const AdjointLayout& A;
     const Tape& tape;
     const KernelArgs& a;
@@ -144,7 +142,7 @@ struct Backward {
     unsigned& seg;  // segment to do next
     float& weight;  // d L / d fitness of the creature
 
-    __device__ __forceinline__ void add_mass(unsigned i, float d) const { b.L.word(A.mass + i / 4u, i % 4u) += d; }
+    __device__ __forceinline__ void add_mass(unsigned i, float d) const { gmass[i * g.stride] += d; }
 
     // d J / d w for an inverse mass w = 1 / m, as d J / d m.
     __device__ __forceinline__ void add_inverse_mass(unsigned i, float w, float dw) const { add_mass(i, -dw * w * w); }
@@ -172,13 +170,13 @@ struct Backward {
         }
         for (unsigned q = 0u; q < (r.nodes + 3u) / 4u; q++) {
             b.L.put(A.fric + q, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
-            b.L.put(A.mass + q, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
         }
         for (unsigned i = 0u; i < r.nodes; i++) {
             const float m = b.L.get(b.S.node + i).x;
             g.pos(i) = make_float2(usable ? weight * m * r.inv_mass : 0.0f, 0.0f);
             g.vel(i) = make_float2(0.0f, 0.0f);
             g.f(i) = make_float2(0.0f, 0.0f);
+            gmass[i * g.stride] = 0.0f;
         }
         for (unsigned k = 0u; k < r.muscles; k++) {
             g.muscle(k) = make_float2(0.0f, 0.0f);
@@ -209,7 +207,7 @@ struct Backward {
         }
         for (unsigned i = 0u; i < r.nodes; i++) {
             out[kGradMuscle * a.mm + i] = b.L.word(A.fric + i / 4u, i % 4u);
-            out[kGradMuscle * a.mm + a.rows + i] = b.L.word(A.mass + i / 4u, i % 4u);
+            out[kGradMuscle * a.mm + a.rows + i] = gmass[i * g.stride];
             // The adjoint of the start position (the tables hold the state's
             // adjoint at the start of the trial once every segment is done).
             const float2 l0 = g.pos(i);
@@ -562,7 +560,9 @@ struct Backward {
             }
             const float4 nr = L.get(S.node + i);
             const float* pj = reinterpret_cast<const float*>(&L.base[(A.pj + i / 2u) * 32u]) + 2u * (i % 2u);
-            ground_back(i, nr, make_float2(pj[0], pj[1]), t.f(i), ((slip >> i) & 1u) != 0u);
+            // The substep's start position, from the tape: the forward
+            // force table and the adjoint force table share memory.
+            ground_back(i, nr, make_float2(pj[0], pj[1]), *tape.pair(k_tape, 2u * i), ((slip >> i) & 1u) != 0u);
         }
         // Joint limits, last to first, on the joints that were pushed.
         for (unsigned j = bones; j-- > 1u;) {
@@ -1044,10 +1044,17 @@ __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, 
     using B = Backward<W, RATE>;
     const unsigned threads = blockDim.x;
     float2* const tables = reinterpret_cast<float2*>(smem) + threadIdx.x;
+    // Tables of rows x threads entries: positions, velocities, the adjoints
+    // of both, one force table (the forward passes' forces and start
+    // positions, then the reverse passes' adjoints of those: each is dead
+    // while the other is in use), the mass gradients (one float an entry),
+    // then the muscles' (energy, demand) pairs and their adjoints.
     const size_t node_table = (size_t)a.rows * threads, muscle_table = (size_t)(a.mm > 0u ? a.mm : 1u) * threads;
-    const NodeTables tab{tables, tables + node_table, tables + 2u * node_table, tables + 6u * node_table, threads};
-    const NodeTables adj{tables + 3u * node_table, tables + 4u * node_table, tables + 5u * node_table,
-                         tables + 6u * node_table + muscle_table, threads};
+    float2* const forces = tables + 4u * node_table;
+    float* const gmass = reinterpret_cast<float*>(reinterpret_cast<float2*>(smem) + 5u * node_table) + threadIdx.x;
+    float2* const muscles = reinterpret_cast<float2*>(smem) + 5u * node_table + node_table / 2u + threadIdx.x;
+    const NodeTables tab{tables, tables + node_table, forces, muscles, threads};
+    const NodeTables adj{tables + 2u * node_table, tables + 3u * node_table, forces, muscles + muscle_table, threads};
     const SlotLayout S = SlotLayout::make(a.rows, a.mm, false);
     const AdjointLayout A = AdjointLayout::make(a.rows, a.mm);
     const unsigned lane = threadIdx.x & 31u;
@@ -1061,7 +1068,7 @@ __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, 
     const typename B::Body body{w, p, tab, L, S, r};
     unsigned end = 0u, seg = 0u;
     float weight = 1.0f;
-    const B back{body, adj, A, tape, a, x, end, seg, weight};
+    const B back{body, adj, gmass, A, tape, a, x, end, seg, weight};
     bool live = false;
     Claim claim(a, lane, warp, warps_total);
     for (;;) {
@@ -1092,7 +1099,7 @@ __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, 
 }  // namespace
 
 size_t adjoint_smem_bytes(unsigned rows, unsigned mm, unsigned block) {
-    return (size_t)block * (rows * 48u + (mm > 0u ? mm : 1u) * 16u);
+    return (size_t)block * (rows * 44u + (mm > 0u ? mm : 1u) * 16u);
 }
 
 size_t adjoint_slot_bytes(unsigned grid, unsigned rows, unsigned mm) {
