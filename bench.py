@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--creatures", type=int, default=3_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-adjoint", action="store_true", help="leave out the gradient measurement")
+    ap.add_argument("--no-effects", action="store_true", help="leave out the effects-world measurement")
     return ap.parse_args()
 
 
@@ -255,6 +256,32 @@ def adjoint_bench(eng) -> dict:
                       "plain submission)"}
 
 
+EFFECTS_TEXT = ("3,000,000 seeded synthetic creatures (seed 2), 3-24 nodes (geometric, mean 7), joint ranges "
+                "+-U(30, 150) deg, rough ground 0.08 m, 1.5 g, thick air, wet grip, 8% slope, headwind, shallows "
+                "0.35 m, ice patches, low hurdles; 20 s trials, FP32")
+
+
+def effects_workload():
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS["effects"]
+    world = w.world()
+    return world, ce.pack(ce.generate(w.spec, w.count), world)
+
+
+def effects_bench(eng) -> dict:
+    """One generation of the effects workload through ce_submit (GPU-busy
+    time of the second of two submissions)."""
+    import evolution_simulator_gpu_b200 as ce
+    world, wave = effects_workload()
+    eng.run(wave, world)
+    res, busy = eng.run(wave, world)
+    units = ce.creature_substeps(res, world)
+    return {"workload": EFFECTS_TEXT, "unit": UNIT, "value": units / busy, "seconds": busy,
+            "creature_substeps": units,
+            "timing": "CUDA events around one submission (bucketing and both size classes)"}
+
+
 # ---------------------------------------------------------------- engine arm
 def run_engine(args):
     world_size, rank, local = dist_setup(args.gpus)
@@ -345,6 +372,7 @@ def run_engine(args):
                     if flops_per else None}
         cpu = cpu_baseline(wave, world, args.cpu_seconds)
         adjoint = adjoint_bench(eng) if not args.no_adjoint else None
+        effects = effects_bench(eng) if not args.no_effects else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -358,7 +386,7 @@ def run_engine(args):
                     "seconds_per_step": e2e_s / args.steps, "timing": "host wall clock around ce_submit+ce_poll",
                     "results_equal_device_path": same},
             "gpu_launches": (BUCKET_KERNELS + 1) * args.steps, "gpu_launches_e2e": e2e_launches,
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "adjoint": adjoint,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "adjoint": adjoint, "effects": effects,
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -415,6 +443,13 @@ def run_reference(args):
                                    "value": len(gwave) / (gms / 1e3 * 2.0 * gparams),
                                    "what": "central finite differences on the reference's kernel: 2 trials a "
                                            "parameter (the reference has no gradients)"}
+        if not args.no_effects:
+            eworld, ewave = effects_workload()
+            ekern = RefKernel(ce.world_flags(eworld), eworld.rate or 60)
+            ekern.run(ewave.take(np.arange(4096)), ce.make_params(eworld))
+            eres, ems = ekern.run(ewave, ce.make_params(eworld))
+            ref_gpu["effects"] = {"workload": EFFECTS_TEXT, "unit": UNIT, "seconds": ems / 1e3,
+                                  "value": ce.creature_substeps(eres, eworld) / (ems / 1e3)}
     except Exception as exc:  # the reference kernel needs a GPU
         ref_gpu = {"unavailable": str(exc).splitlines()[0]}
     sample = (f"{tot_count} creatures of the generation (chunks spread over the packed order), "
