@@ -476,7 +476,7 @@ class Engine:
                  small_body: int = 0):
         """`ctas_per_sm` (0: as many as fit), `chunk_k` (creatures a warp
         claims per queue visit, 0: 4) and `small_body` (largest node count run
-        as a small body, 0: 16) are the launch shape; `autotune` picks them."""
+        as a small body, 0: 12) are the launch shape; `autotune` picks them."""
         h = C.c_void_p()
         opts = Options(slots, ctas_per_sm, 0, chunk_k, small_body)
         _check(lib().ce_open(device, C.byref(opts), C.byref(h)), "ce_open")

@@ -29,7 +29,7 @@ using ce::set_error;
 namespace {
 
 // Bodies of up to this many nodes form the first size class (default).
-constexpr unsigned kSmallBody = 16u;
+constexpr unsigned kSmallBody = 12u;
 
 ce_status cuda_status(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return CE_OK;
