@@ -112,6 +112,25 @@ def _record_change(wa, wb, h):
     return dm, dn, dmass, ds
 
 
+def test_adjoint_at_the_fine_rate_matches_fp64_tangent(engine):
+    """The 120 steps/s kernels (the reference's fine fidelity): the adjoint
+    against the FP64 tangent along random record directions."""
+    world = W.world(duration=0.05, rate=120)
+    wave = ce.pack(ce.generate(W.spec, 256), world)
+    with engine.forward(wave, world) as tape:
+        g = tape.backward()
+        rows, mm = tape.shape
+        res = tape.results
+    dm, dn, dmass, ds = _record_direction(wave, rows, mm, np.random.default_rng(9))
+    tangent, _, _ = Oracle().tangent(wave, ce.make_params(world), ce.world_flags(world), dm, dn, rate=120,
+                                     dmass=dmass)
+    adj = _project(g, rows, mm, dm, dn, dmass, ds)
+    ok = res["fitness"] > -1e19
+    rel = np.abs(adj - tangent)[ok] / np.maximum(np.abs(tangent[ok]), 1e-12)
+    assert np.median(rel) < 1e-4, np.median(rel)
+    assert (rel < 1e-3).mean() >= 0.9, (rel < 1e-3).mean()
+
+
 @pytest.mark.parametrize("name,count,seconds", [("gradients", 64, 0.1), ("refine", 384, 0.05)])
 def test_gene_gradients_match_fp64_differences(engine, name, count, seconds):
     """End to end: GPU record gradient, gene chain rule, against central
