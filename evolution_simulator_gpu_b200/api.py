@@ -536,14 +536,14 @@ class Engine:
         if not pending:
             return None
         cap = max(pending.values())
-        out = np.zeros(cap, RESULT_DTYPE)
+        out = np.empty(cap, RESULT_DTYPE)  # the library fills the first n
         t, n, busy = C.c_uint64(), C.c_size_t(), C.c_double()
         st = lib().ce_poll(self.handle, int(timeout_s * 1e6), C.byref(t), _ptr(out), cap, C.byref(n), C.byref(busy))
         if st == CE_ERR_TIMEOUT:
             return None
         _check(st, "ce_poll")
         pending.pop(t.value, None)
-        return t.value, out[:n.value].copy(), busy.value
+        return t.value, (out if n.value == cap else out[:n.value].copy()), busy.value
 
     def wait(self, timeout_s: float) -> bool:
         st = lib().ce_wait(self.handle, int(timeout_s * 1e6))

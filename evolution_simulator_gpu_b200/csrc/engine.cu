@@ -1118,7 +1118,7 @@ extern "C" ce_status ce_autotune(ce_engine* e, const ce_wave_pack* sample, const
     unsigned best_cta = keep_cta, best_chunk = keep_chunk, best_small = keep_small;
     for (unsigned cta : {0u, 3u}) {
         for (unsigned chunk : {2u, 4u, 8u}) {
-            for (unsigned small : {12u, 16u, 24u}) {
+            for (unsigned small : {10u, 12u, 16u, 24u}) {
                 e->ctas_per_sm = cta;
                 e->chunk_k = chunk;
                 e->small_body = small;
