@@ -73,7 +73,8 @@ def main() -> None:
         w = WORKLOADS[args.workload]
         with ce.Engine(0) as eng:
             out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
-                                count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler)
+                                count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler,
+                                guided=True)
         out.update(workload=args.workload, seconds=args.seconds)
         print(json.dumps(out))
         return

@@ -254,7 +254,7 @@ def _evaluate(engine, pop, world, chunk: int):
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
            resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None,
-           sampler: str = "host") -> dict:
+           sampler: str = "host", guided: bool = False) -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -273,7 +273,10 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     (fitness, sample) pairs), and each rank refines and resamples the elites
     among its own samples; the report's figures are totals over the ranks,
     the same on every rank. `sampler` "device" draws the samples on the GPU
-    (samples_gpu), "host" with numpy (samples)."""
+    (samples_gpu), "host" with numpy (samples). With `guided`, a third arm
+    spends the same GPU time on one gradient of each elite (the
+    refinement's first forward and backward run) and children drawn around
+    the elite moved by one ascent step instead of around the elite."""
     draw = samples if sampler == "host" else samples_gpu
     report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
                   ranks=world_size, sampler=sampler)
@@ -294,6 +297,7 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     x = elite
     refine_s = 0.0
     first_equal = True
+    stepped, grad_s = None, 0.0
     t0 = time.perf_counter()
     for k in range(steps if len(mine) else 0):
         wave = api.pack(x, world)
@@ -309,6 +313,8 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
         mg, ng = api.gene_gradients(x, wave, world, g, shape)
         x = ascend(x, mg, ng, step)
+        if k == 0:
+            stepped, grad_s = x, fwd + bwd
     last_s = 0.0
     if len(mine):
         fk, last_s = _evaluate(engine, x, world, chunk)
@@ -323,27 +329,43 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     gain = (tot[2] - tot[1]) / n_el
     report["refine"] = dict(first_equal=bool(tot[6] == 0.0), gpu_s=float(tot[5]), mean_best=tot[2] / n_el, gain=gain,
                             gain_per_gpu_s=gain / tot[5], improved=tot[3] / n_el, host_s=host_refine)
-    if resample:
-        # Rounds of children (one child per elite a round, `rounds` rounds a
-        # batch) until this rank has spent its refinement's GPU time.
-        t0 = time.perf_counter()
+    def resample_around(centres, budget, stream):
+        """Rounds of children around `centres` (one child per elite a round)
+        until `budget` GPU seconds are spent: (best per elite, seconds,
+        rounds)."""
         bestr = f0.copy()
         secs = 0.0
         per = 0
         rounds = max(1, min(chunk, 1 << 19) // max(len(mine), 1))
-        while len(mine) and secs < refine_s:
+        while len(mine) and secs < budget:
             n = rounds * len(mine)
-            # A stream of its own for every rank and batch.
-            kids, parent = draw(elite, n, sigma, (seed + 1) * 10 ** 6 + rank * 10 ** 3 + per // rounds)
+            # A stream of its own for every arm, rank and batch.
+            kids, parent = draw(centres, n, sigma, (seed + stream) * 10 ** 6 + rank * 10 ** 3 + per // rounds)
             # Children keep their elite's id, so they see its tremor phase.
             kids.genomes["id"] = elite.genomes["id"][parent]
             fk, busy_r = _evaluate(engine, kids, world, chunk)
             secs += busy_r
             per += rounds
             np.maximum.at(bestr, parent, np.where(fk > -1e19, fk, -np.inf).astype(np.float64))
+        return bestr, secs, per
+
+    if resample:
+        t0 = time.perf_counter()
+        bestr, secs, per = resample_around(elite, refine_s, 1)
         tr = shard.all_sum([bestr.sum(), (bestr > f0).sum(), secs, per], world_size, group, device)
         gain_r = (tr[0] - tot[1]) / n_el
-        report["resample"] = dict(children_per_elite=tr[3] / world_size, gpu_s=tr[2], mean_best=tr[0] / n_el, gain=gain_r,
-                                  gain_per_gpu_s=gain_r / tr[2], improved=tr[1] / n_el,
+        report["resample"] = dict(children_per_elite=tr[3] / world_size, gpu_s=tr[2], mean_best=tr[0] / n_el,
+                                  gain=gain_r, gain_per_gpu_s=gain_r / tr[2], improved=tr[1] / n_el,
                                   host_s=time.perf_counter() - t0)
+    if guided:
+        t0 = time.perf_counter()
+        if stepped is None:
+            bestg, secs, per = f0.copy(), 0.0, 0
+        else:
+            bestg, secs, per = resample_around(stepped, refine_s - grad_s, 2)
+        tg = shard.all_sum([bestg.sum(), (bestg > f0).sum(), secs + grad_s, per], world_size, group, device)
+        gain_g = (tg[0] - tot[1]) / n_el
+        report["guided"] = dict(children_per_elite=tg[3] / world_size, gpu_s=tg[2], mean_best=tg[0] / n_el,
+                                gain=gain_g, gain_per_gpu_s=gain_g / max(tg[2], 1e-12), improved=tg[1] / n_el,
+                                host_s=time.perf_counter() - t0)
     return report

@@ -13,10 +13,11 @@ pytestmark = pytest.mark.gpu
 
 def test_small_refined_search(engine):
     w = WORKLOADS["refine"]
-    rep = refine.search(engine, w.spec, w.world(duration=1.0), parents=32, count=4096, elites=256, steps=2)
-    r, s = rep["refine"], rep["resample"]
+    rep = refine.search(engine, w.spec, w.world(duration=1.0), parents=32, count=4096, elites=256, steps=2,
+                        guided=True)
+    r, s, g = rep["refine"], rep["resample"], rep["guided"]
     assert r["first_equal"] is True
     assert np.isfinite(rep["elite_mean_fitness"])
-    for arm in (r, s):
+    for arm in (r, s, g):
         assert arm["gpu_s"] > 0 and arm["gain"] >= 0 and np.isfinite(arm["gain_per_gpu_s"])
     assert s["children_per_elite"] >= 1
