@@ -475,7 +475,7 @@ class Engine:
     def __init__(self, device: int = 0, slots: int = 0, ctas_per_sm: int = 0, chunk_k: int = 0,
                  small_body: int = 0):
         """`ctas_per_sm` (0: as many as fit), `chunk_k` (creatures a warp
-        claims per queue visit, 0: 16) and `small_body` (largest node count run
+        claims per queue visit, 0: 64) and `small_body` (largest node count run
         as a small body, 0: 12) are the launch shape; `autotune` picks them."""
         h = C.c_void_p()
         opts = Options(slots, ctas_per_sm, 0, chunk_k, small_body)

@@ -110,7 +110,7 @@ struct ce_engine {
     int device = 0;
     int sms = 0;
     unsigned ctas_per_sm = 0;  // 0: from the occupancy of each kernel
-    unsigned chunk_k = 16;
+    unsigned chunk_k = 64;
     size_t smem_optin = 0;  // shared memory a block may use
     unsigned small_body = kSmallBody;
     std::vector<Slot> slots;
@@ -1117,7 +1117,7 @@ extern "C" ce_status ce_autotune(ce_engine* e, const ce_wave_pack* sample, const
     double best_s = 1e300;
     unsigned best_cta = keep_cta, best_chunk = keep_chunk, best_small = keep_small;
     for (unsigned cta : {0u, 3u}) {
-        for (unsigned chunk : {4u, 8u, 16u}) {
+        for (unsigned chunk : {16u, 32u, 64u}) {
             for (unsigned small : {10u, 12u, 16u, 24u}) {
                 e->ctas_per_sm = cta;
                 e->chunk_k = chunk;

@@ -343,7 +343,7 @@ typedef struct ce_options {
     uint32_t slots;          /* concurrent submissions, 0 = default (4) */
     uint32_t ctas_per_sm;    /* resident blocks an SM, 0 = as many as fit */
     uint32_t warps_per_cta;  /* reserved, 0 (blocks are 4 warps) */
-    uint32_t chunk_k;        /* claims shrink to 1/chunk_k of a queue's rest a warp, 0 = 16 */
+    uint32_t chunk_k;        /* claims shrink to 1/chunk_k of a queue's rest a warp, 0 = 64 */
     uint32_t small_body;     /* most nodes of the first size class, 0 = 12 */
     uint32_t reserved[3];
 } ce_options;

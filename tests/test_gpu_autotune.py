@@ -20,7 +20,7 @@ def test_autotune_keeps_a_grid_setting_and_results(engine):
     with ce.Engine(0) as tuned:
         best, secs = tuned.autotune(sample, world)
         assert best["ctas_per_sm"] in (0, 3)
-        assert best["chunk_k"] in (4, 8, 16)
+        assert best["chunk_k"] in (16, 32, 64)
         assert best["small_body"] in (10, 12, 16, 24)
         assert secs > 0
         got, _ = tuned.run(wave, world)
