@@ -67,17 +67,7 @@ def main() -> None:
     if args.adjoint:
         return adjoint(args)
     if args.refine:
-        import evolution_simulator_gpu_b200 as ce
-        from evolution_simulator_gpu_b200 import refine
-        from evolution_simulator_gpu_b200.configs import WORKLOADS
-        w = WORKLOADS[args.workload]
-        with ce.Engine(0) as eng:
-            out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
-                                count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler,
-                                guided=True)
-        out.update(workload=args.workload, seconds=args.seconds)
-        print(json.dumps(out))
-        return
+        return refined(args)
     import evolution_simulator_gpu_b200 as ce
     from evolution_simulator_gpu_b200.configs import WORKLOADS
     w = WORKLOADS[args.workload]
@@ -97,6 +87,39 @@ def main() -> None:
         out["reference_s"] = ms / 1e3
         out["bit_equal"] = bool((mine.view(np.uint32) == ref.view(np.uint32)).all())
     print(json.dumps(out))
+
+
+def refined(args) -> None:
+    """One refined search generation; under torchrun, over one GPU a rank
+    (rank r draws and evaluates its share of the samples, the elites are
+    chosen over all ranks and each rank refines its own)."""
+    import os
+    from datetime import timedelta
+
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200 import refine
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    world_size, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+    device = None
+    if world_size > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        device = torch.device("cuda", local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+    w = WORKLOADS[args.workload]
+    try:
+        with ce.Engine(local) as eng:
+            out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
+                                count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler,
+                                guided=True, rank=rank, world_size=world_size, device=device)
+    finally:
+        if world_size > 1:
+            dist.destroy_process_group()
+    out.update(workload=args.workload, seconds=args.seconds)
+    if rank == 0:
+        print(json.dumps(out))
 
 
 def adjoint(args) -> None:

@@ -162,14 +162,14 @@ def samples(parents: api.Population, count: int, sigma: float, seed: int, first_
 
 
 def samples_gpu(parents: api.Population, count: int, sigma: float, seed: int, first_id: int = 1, first: int = 0,
-                device: int = 0):
+                device=None):
     """Samples [first, first + count) drawn on the GPU (ce_sample_device):
     the moves of `samples`, from a counter-based hash of (seed, sample, gene,
-    field) instead of numpy's streams. Returns (population on the host,
-    parent of each sample)."""
+    field) instead of numpy's streams, on GPU `device` (the current one by
+    default). Returns (population on the host, parent of each sample)."""
     import torch
     import ctypes as C
-    dev = torch.device("cuda", device)
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
     par = take(parents, np.arange(len(parents)))  # genes packed in order from row 0
 
     def up(arr):
