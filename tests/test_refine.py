@@ -95,3 +95,19 @@ def test_ascent_step_follows_the_gradient_within_its_clip():
     # Non-finite gradients do not move a coordinate.
     bad = refine.ascend(pop, np.full_like(gm, np.nan), np.full_like(gn, np.inf), 1e-2)
     assert _same(bad.nodes, pop.nodes)
+
+
+def test_host_samples_do_not_depend_on_the_range():
+    """A sample's moves come from its block's own stream: drawing samples
+    [0, 10000) at once or as [0, 3000) and [3000, 10000) gives the same
+    genes, as the ranks of a split search rely on."""
+    parents = ce.generate(W.spec, 100)
+    whole, parent = refine.samples(parents, 10_000, 0.05, seed=4)
+    a, pa = refine.samples(parents, 3000, 0.05, seed=4)
+    b, pb = refine.samples(parents, 7000, 0.05, seed=4, first=3000)
+    joined = refine.concat([a, b])
+    for f in ("nodes", "bones", "muscles", "genomes", "strength"):
+        assert _same(getattr(whole, f), getattr(joined, f)), f
+    assert (np.concatenate([pa, pb]) == parent).all()
+    other, _ = refine.samples(parents, 10_000, 0.05, seed=5)
+    assert not (other.nodes["x"] == whole.nodes["x"]).all()
