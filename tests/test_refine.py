@@ -111,3 +111,18 @@ def test_host_samples_do_not_depend_on_the_range():
     assert (np.concatenate([pa, pb]) == parent).all()
     other, _ = refine.samples(parents, 10_000, 0.05, seed=5)
     assert not (other.nodes["x"] == whole.nodes["x"]).all()
+
+
+def test_sample_rows_count_the_tiled_parents():
+    """ce_sample_rows (the device sampler's output sizes): samples
+    [first, first + count) of P parents hold the rows of parents
+    first mod P, ..., (first + count - 1) mod P."""
+    import ctypes as C
+    parents = ce.generate(W.spec, 37)
+    g = parents.genomes
+    for first, count in ((0, 100), (5, 1), (36, 74), (1000, 333), (0, 0)):
+        idx = (first + np.arange(count)) % len(parents)
+        rows = [C.c_size_t() for _ in range(3)]
+        assert ce.lib().ce_sample_rows(ce.api._ptr(g), len(parents), first, count, *[C.byref(r) for r in rows]) == 0
+        want = [int(g[f][idx].sum()) for f in ("node_count", "bone_count", "muscle_count")]
+        assert [r.value for r in rows] == want
