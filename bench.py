@@ -380,6 +380,8 @@ def run_engine(args):
             "config": {"workload": WORKLOAD_TEXT, "creatures_per_gpu": len(wave),
                        "trial_steps": ce.trial_steps(world), "substeps_per_step": 16,
                        "mean_steps_run": units / 16.0 / len(wave),
+                       "nominal_creature_substeps": len(wave) * ce.trial_steps(world) * 16,
+                       "trials_ended_early": float(((res["fall_time"] > 0) | (res["screened"] > 0)).mean()),
                        "l2": "inputs larger than L2 (%.1f GB of packed records per GPU)" % (h2d / 1e9),
                        "parallelism": f"dp{world_size} (independent generations per GPU)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
