@@ -329,6 +329,7 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     gain = (tot[2] - tot[1]) / n_el
     report["refine"] = dict(first_equal=bool(tot[6] == 0.0), gpu_s=float(tot[5]), mean_best=tot[2] / n_el, gain=gain,
                             gain_per_gpu_s=gain / tot[5], improved=tot[3] / n_el, host_s=host_refine)
+
     def resample_around(centres, budget, stream):
         """Rounds of children around `centres` (one child per elite a round)
         until `budget` GPU seconds are spent: (best per elite, seconds,
