@@ -21,6 +21,7 @@ Under torchrun each rank evaluates its own generation (weak scaling).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -162,6 +163,13 @@ def build_workload(n: int, rank: int):
     pop = ce.generate(w.spec, n, first=rank * n)
     wave = ce.pack(pop, world)
     return world, pop, wave
+
+
+def results_digest(res) -> str:
+    """SHA-256 of a generation's result words in packed order: the engine arm
+    and the reference arm print it for the same generation, so equal digests
+    show the two kernels' results equal to the bit."""
+    return hashlib.sha256(np.ascontiguousarray(res).view(np.uint8).tobytes()).hexdigest()
 
 
 def op_counts() -> dict:
@@ -386,7 +394,10 @@ def run_engine(args):
                        "parallelism": f"dp{world_size} (independent generations per GPU)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s / args.steps, "timing": "host wall clock around ce_submit+ce_poll",
-                    "results_equal_device_path": same},
+                    "results_equal_device_entry": same},
+            "parity": {"results_sha256": results_digest(res),
+                       "compare_with": "the reference arm's reference_gpu.results_sha256: the reference kernel's "
+                                       "results for the same generation in the same packed order"},
             "gpu_launches": (BUCKET_KERNELS + 1) * args.steps, "gpu_launches_e2e": e2e_launches,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "adjoint": adjoint, "effects": effects,
         }
@@ -434,6 +445,7 @@ def run_reference(args):
         kern.run(wave.take(np.arange(4096)), params)
         res, ms = kern.run(wave, params)
         ref_gpu = {"value": ce.creature_substeps(res, world) / (ms / 1e3), "unit": UNIT,
+                   "results_sha256": results_digest(res),
                    "what": "the reference's own kernel (shaders/creature.cu) built for sm_100a with its NVRTC "
                            "options, launched with its engine's wave and grid rule, CUDA-event time of one "
                            "generation", "seconds": ms / 1e3}

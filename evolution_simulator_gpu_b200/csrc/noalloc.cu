@@ -15,9 +15,11 @@
 // bodies, so this entry point can be slower than ce_advance_device); a body
 // size whose single block does not fit is rejected. Every call shares the
 // array: calls whose work overlaps on the GPU (two streams, or two host
-// threads) race on it and must not be issued. The first call on a device
-// resolves the array's address there; make that first call before any stream
-// capture.
+// threads) race on it and must not be issued. Each call outside a stream
+// capture looks the array's address up on the current device (so it stays
+// right after the host recreates the device's primary context); a call
+// inside a capture reuses the address of the last call outside one, so the
+// first call on a device must come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,14 +41,25 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
 
-// The array's device address on the current device, resolved once per device.
-ce_status scratch_address(int device, void** out) {
+// The array's device address on the current device. Outside a stream
+// capture it is looked up on every call, so a primary context that the host
+// tore down and created again (cudaDeviceReset, which reloads the library's
+// module at a new address) is followed; inside a capture the address that
+// the last call outside a capture found is used, since a capture must not
+// be broken by a lookup.
+ce_status scratch_address(int device, cudaStream_t stream, void** out) {
     std::lock_guard<std::mutex> lock(g_mutex);
     if (device < 0 || device >= kMaxDevices) {
         ce::set_error("ce_advance_device_noalloc: device ordinal out of range");
         return CE_ERR_INVALID;
     }
-    if (!g_scratch_addr[device]) {
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    const cudaError_t q = cudaStreamIsCapturing(stream, &capture);
+    if (q != cudaSuccess) {
+        ce::set_error(std::string("ce_advance_device_noalloc: cudaStreamIsCapturing: ") + cudaGetErrorString(q));
+        return CE_ERR_DEVICE;
+    }
+    if (capture == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -54,6 +67,9 @@ ce_status scratch_address(int device, void** out) {
             return CE_ERR_DEVICE;
         }
         g_scratch_addr[device] = p;
+    } else if (!g_scratch_addr[device]) {
+        ce::set_error("ce_advance_device_noalloc: the first call on a device must come before any stream capture");
+        return CE_ERR_INVALID;
     }
     *out = g_scratch_addr[device];
     return CE_OK;
@@ -83,7 +99,7 @@ extern "C" ce_status ce_advance_device_noalloc(const uint32_t* records, const fl
         return CE_ERR_DEVICE;
     }
     void* base = nullptr;
-    ce_status s = scratch_address(device, &base);
+    ce_status s = scratch_address(device, static_cast<cudaStream_t>(stream), &base);
     if (s != CE_OK) return s;
     // Warps whose slots fit in the array at this body size.
     const size_t warp_bytes = (size_t)cek::slot_lines(max_nodes, max_muscles, false) * 32u * 16u;

@@ -470,8 +470,11 @@ ce_status ce_gene_gradients(const ce_population* pop, const uint32_t* indices, s
  * device, as many warps as the array holds at this body size (so it can be
  * slower than ce_advance_device), and rejects a body size whose single block
  * does not fit. Calls share the array: calls that overlap on the GPU race.
- * The first call on a device resolves the array's address there and must
- * come before any stream capture. Inputs and outputs are the caller's. */
+ * A call outside a stream capture looks the array's address up on the
+ * current device each time (so a primary context that was torn down and
+ * created again is followed); a call inside a capture reuses the address
+ * the last call outside one found, so the first call on a device must come
+ * before any stream capture. Inputs and outputs are the caller's. */
 ce_status ce_advance_device_noalloc(const uint32_t* records, const float* muscles,
                                     const uint32_t* heads, ce_result* results,
                                     const ce_params* params, uint32_t world_flags, uint32_t rate,

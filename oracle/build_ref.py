@@ -10,6 +10,10 @@
 2. The CPU oracle (oracle/creature_oracle.cpp) into oracle/_ref/liboracle.so.
 
     python oracle/build_ref.py [--reference PATH] [--force]
+
+The reference checkout is found at --reference, else at the directory the
+REFERENCE_DIR environment variable names, else at a checkout called
+`reference` beside this repository's folder.
 """
 from __future__ import annotations
 
@@ -23,7 +27,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REFERENCE = Path("/root/reference")
+DEFAULT_REFERENCE = Path(os.environ.get("REFERENCE_DIR") or HERE.parent.parent / "reference")
 
 FLAG_NAMES = ["GROUND", "TERRAIN", "SLOPE", "GAPS", "HURDLES", "QUAKE", "MUD", "WATER", "ICE", "WIND", "AIR",
               "BRAMBLES"]

@@ -1,16 +1,14 @@
-"""A small, GPU-filling evaluation for profilers (ncu), and a timing check
-of the engine against the reference kernel on the same case.
+"""A small, GPU-filling evaluation for profilers (ncu): the bench's workloads
+at sizes an ncu capture finishes in a minute or two.
 
-    python -m evolution_simulator_gpu_b200.profile_case --workload game \
-        --creatures 300000 --seconds 1 [--reference]
-    python -m evolution_simulator_gpu_b200.profile_case --workload effects \
+    python profile_case.py --workload game \
+        --creatures 300000 --seconds 1
+    python profile_case.py --workload effects \
         --creatures 3000000 --seconds 20 --generations 10 --autotune
 
 It generates the workload, runs one submission through the engine (one
 launch per size class) and prints the GPU seconds, the creature-substeps the
-trials ran and the bytes of the packed records. With --reference it also
-runs the reference's own kernel (oracle/_ref, built from its source) on the
-same batch and prints whether the results are equal to the bit.
+trials ran and the bytes of the packed records.
 
 With --generations K it packs K generations of the workload (disjoint
 creature ranges), keeps them resident and runs them as one CUDA graph
@@ -29,7 +27,7 @@ With --refine it runs one gradient-refined search generation (refine.py):
 --steps adjoint ascent steps, against plain resampling of the same elites
 for the same GPU time, and prints the fitness gained per GPU-second of both.
 
-    python -m evolution_simulator_gpu_b200.profile_case --workload refine \
+    python profile_case.py --workload refine \
         --refine --creatures 1000000 --parents 1024 --elites 16384 --steps 5 --seconds 20
 """
 from __future__ import annotations
@@ -41,7 +39,9 @@ from pathlib import Path
 
 import numpy as np
 
-ROOT = Path(__file__).resolve().parent.parent
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
 
 
 def main() -> None:
@@ -49,7 +49,6 @@ def main() -> None:
     ap.add_argument("--workload", default="game")
     ap.add_argument("--creatures", type=int, default=300_000)
     ap.add_argument("--seconds", type=float, default=1.0)
-    ap.add_argument("--reference", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="resident blocks per SM (0: the engine's choice)")
     ap.add_argument("--generations", type=int, default=0, help="run K resident generations as one CUDA graph")
     ap.add_argument("--autotune", action="store_true", help="tune the launch shape on a sample first")
@@ -80,12 +79,6 @@ def main() -> None:
            "ctas_per_sm": args.ctas_per_sm, "engine_s": busy,
            "creature_substeps": ce.creature_substeps(mine, world),
            "record_bytes": int(wave.lanes.nbytes + wave.muscles.nbytes + wave.heads.nbytes)}
-    if args.reference:
-        sys.path.insert(0, str(ROOT))
-        from oracle.ref import RefKernel
-        ref, ms = RefKernel(ce.world_flags(world), world.rate or 60).run(wave, ce.make_params(world))
-        out["reference_s"] = ms / 1e3
-        out["bit_equal"] = bool((mine.view(np.uint32) == ref.view(np.uint32)).all())
     print(json.dumps(out))
 
 

@@ -46,3 +46,20 @@ def test_errors_are_reported_without_a_gpu():
     assert lib.ce_free_slots(None) == 0
     assert lib.ce_allocated_bytes(None) == 0
     del h
+
+
+def test_failure_entry_points_reject_null_handles_without_a_gpu():
+    lib = ce.lib()
+    assert lib.ce_inject_fault(None, 1, ce.CE_ERR_DEVICE) == ce.CE_ERR_INVALID
+    assert lib.ce_wait(None, 0) == ce.CE_ERR_INVALID
+    assert lib.ce_release_idle(None) == ce.CE_ERR_INVALID
+    t, n, busy = C.c_uint64(), C.c_size_t(), C.c_double()
+    assert lib.ce_poll(None, 0, C.byref(t), None, 0, C.byref(n), C.byref(busy)) == ce.CE_ERR_INVALID
+    assert lib.ce_close(None) == ce.CE_OK
+    h = C.c_void_p()
+    assert lib.ce_open(0, None, None) == ce.CE_ERR_INVALID
+    # With no GPU (or a device ordinal that does not exist) the open fails
+    # with a status and a message, never a crash.
+    st = lib.ce_open(1000, None, C.byref(h))
+    assert st != ce.CE_OK and not h.value
+    assert lib.ce_last_error()
