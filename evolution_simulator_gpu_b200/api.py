@@ -170,6 +170,9 @@ def _bind(lib: C.CDLL) -> None:
         "ce_advance_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, P(Params), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p]),
+        "ce_advance_device_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, P(Params), P(World), C.c_uint32, C.c_uint32,
+                                              C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
         "ce_measure_fp32": (C.c_int, [C.c_int, P(C.c_double), P(C.c_double)]),
         "ce_ground": (None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P(C.c_float),
@@ -229,7 +232,7 @@ def lib() -> C.CDLL:
 EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_frame_stride", "ce_generate_size",
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
-            "ce_advance_scratch_bytes", "ce_advance_device", "ce_inject_fault", "ce_measure_fp32",
+            "ce_advance_scratch_bytes", "ce_advance_device", "ce_advance_device_cells", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
@@ -602,6 +605,18 @@ class Engine:
         _check(lib().ce_advance_device(self.handle, records, muscles, heads, results, counter, scratch,
                                        C.byref(params), flags, rate, max_nodes, max_muscles, stream or None),
                "ce_advance_device")
+
+    def advance_device_cells(self, records: int, muscles: int, heads: int, results: int, counter: int, scratch: int,
+                             params: Params, world: World, max_nodes: int, max_muscles: int, shapes: int,
+                             cells: int, metrics: int = 0, stream: int = 0, global_layout: bool = True) -> None:
+        """advance_device with the niche epilogue in the creature kernel:
+        each trial's metrics row (METRICS_DTYPE at `metrics`, 0 for none)
+        and dense niche cell (int64 at `cells`) are stored with its result;
+        `shapes` holds shape_classes() of the packed batch (asynchronous)."""
+        _check(lib().ce_advance_device_cells(self.handle, records, muscles, heads, results, counter, scratch,
+                                             C.byref(params), C.byref(world), max_nodes, max_muscles, shapes,
+                                             1 if global_layout else 0, metrics or None, cells, stream or None),
+               "ce_advance_device_cells")
 
 
 # ------------------------------------------------------------------ graphs

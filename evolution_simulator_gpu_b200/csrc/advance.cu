@@ -20,9 +20,17 @@ static int carveout_for(size_t smem, int blocks) {
     return pct < 1 ? 1 : (pct > 100 ? 100 : pct);
 }
 
+// The kernel of a world, recording switch and step rate: the plain kernel
+// keeps its node, bone and joint constants in TMEM, the recording kernel in
+// the lanes' lines.
+template <class W, bool RECORD, int RATE>
+constexpr auto kernel_of() {
+    return advance_kernel<W, RECORD, RATE, false, !RECORD>;
+}
+
 template <class W, bool RECORD, int RATE>
 static cudaError_t occupancy_one(unsigned rows, unsigned mm, unsigned block, int* blocks) {
-    auto kern = advance_kernel<W, RECORD, RATE>;
+    auto kern = kernel_of<W, RECORD, RATE>();
     const size_t smem = smem_bytes(rows, mm, block);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -33,7 +41,7 @@ static cudaError_t occupancy_one(unsigned rows, unsigned mm, unsigned block, int
 
 template <class W, bool RECORD, int RATE>
 static cudaError_t launch_one(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const W& w) {
-    auto kern = advance_kernel<W, RECORD, RATE>;
+    auto kern = kernel_of<W, RECORD, RATE>();
     const size_t smem = smem_bytes(s.rows, s.mm, s.block);
     int blocks = 0;
     cudaError_t e = occupancy_one<W, RECORD, RATE>(s.rows, s.mm, s.block, &blocks);
@@ -41,7 +49,12 @@ static cudaError_t launch_one(const LaunchSpec& s, const KernelArgs& a, const ce
     e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                              carveout_for(smem, blocks > 0 ? blocks : 1));
     if (e != cudaSuccess) return e;
-    kern<<<s.grid, s.block, smem, s.stream>>>(a, p, w);
+    KernelArgs args = a;
+    // TMEM columns of a block: an even share of the 512 among the blocks that
+    // can sit on a multiprocessor at once, so no block waits for columns.
+    const unsigned share = s.sm_share ? s.sm_share : (unsigned)(blocks > 0 ? blocks : 1);
+    args.tmem_cols = tmem_columns(TmLayout::make(s.rows, w.has(CE_FLAG_WATER)).total, share);
+    kern<<<s.grid, s.block, smem, s.stream>>>(args, p, w);
     return cudaGetLastError();
 }
 
@@ -81,7 +94,7 @@ cudaError_t advance_reserve_smem(unsigned rows, unsigned mm, uint32_t flags, boo
         constexpr bool R = decltype(rec_tag)::value;
         constexpr int RT = decltype(rate_tag)::value;
         return by_world<R, RT>(flags, [&](auto w) {
-            return cudaFuncSetAttribute(advance_kernel<decltype(w), R, RT>,
+            return cudaFuncSetAttribute(kernel_of<decltype(w), R, RT>(),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         });
     };
@@ -114,4 +127,36 @@ cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool r
 
 namespace cek {
 unsigned slot_lines(unsigned rows, unsigned mm, bool record) { return SlotLayout::make(rows, mm, record).lines; }
+
+// Transpose of a rows x creatures matrix of float2 into creatures x rows,
+// 32 x 32 tiles through shared memory (the extra column keeps the tile's
+// column reads free of bank conflicts), both sides read and written as
+// coalesced rows. Tiles are taken by a grid-stride loop.
+__global__ void __launch_bounds__(256) frames_transpose(const float2* __restrict__ src, float2* __restrict__ dst,
+                                                        size_t rows, uint32_t creatures) {
+    __shared__ float2 tile[32][33];
+    const size_t tiles_r = (rows + 31u) / 32u, tiles_c = (creatures + 31u) / 32u;
+    for (size_t tile_i = blockIdx.x; tile_i < tiles_r * tiles_c; tile_i += gridDim.x) {
+        const size_t r0 = (tile_i / tiles_c) * 32u, c0 = (tile_i % tiles_c) * 32u;
+        for (unsigned y = threadIdx.y; y < 32u; y += 8u) {
+            const size_t r = r0 + y, c = c0 + threadIdx.x;
+            if (r < rows && c < creatures) tile[y][threadIdx.x] = src[r * creatures + c];
+        }
+        __syncthreads();
+        for (unsigned y = threadIdx.y; y < 32u; y += 8u) {
+            const size_t c = c0 + y, r = r0 + threadIdx.x;
+            if (r < rows && c < creatures) dst[c * rows + r] = tile[threadIdx.x][y];
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_frames_to_creature_major(const float2* src, float2* dst, size_t rows, uint32_t creatures,
+                                            cudaStream_t stream) {
+    const size_t tiles = ((rows + 31u) / 32u) * ((creatures + 31u) / 32u);
+    const unsigned grid = (unsigned)(tiles < 148u * 16u ? tiles : 148u * 16u);
+    if (grid == 0u) return cudaSuccess;
+    frames_transpose<<<grid, dim3(32, 8), 0, stream>>>(src, dst, rows, creatures);
+    return cudaGetLastError();
+}
 }  // namespace cek

@@ -18,20 +18,49 @@
 #pragma once
 #include "kernels.h"
 #include "physics.cuh"
+#include "tmem.cuh"
 
 namespace cek {
 
 constexpr uint32_t kChunk = 32;
 
-// Per-lane values kept in registers across a step.
+// Per-lane values kept in registers across a step. `wn` is the most nodes
+// of any live lane of the warp (the same on every lane), the trip count of
+// the passes whose constants come from TMEM.
 struct LaneRegs {
-    uint32_t nodes, muscles, feet, cidx, step, flags, rec_slot;
+    uint32_t nodes, muscles, feet, cidx, step, flags, rec_slot, wn;
     float amp, qphase, inv_mass, period_f;
     bool limp, scoring;
 };
 
+// A warp's TMEM constants (tmem.cuh): where each kind lives and whether all
+// of that kind fit in the block's columns. A kind that does not fit is read
+// from the lane's lines instead, as without TMEM.
+struct TmView {
+    Tmem tm;
+    TmLayout lay;
+    bool nodes, bones, joints, limits, hubs, radii;
+    __device__ __forceinline__ static TmView make(const Tmem& tm, unsigned ns, bool water) {
+        TmView v;
+        v.tm = tm;
+        v.lay = TmLayout::make(ns, water);
+        v.nodes = v.lay.bone <= tm.cols;
+        v.bones = v.lay.joint <= tm.cols;
+        v.joints = v.lay.limit <= tm.cols;
+        v.limits = v.lay.hub <= tm.cols;
+        v.hubs = v.lay.radius <= tm.cols;
+        v.radii = water && v.lay.total <= tm.cols;
+        return v;
+    }
+};
+
 // ------------------------------------------------------ substep passes
-template <class W, int RATE, bool RECORD>
+// TM: the node, bone and joint constants of the substep passes come from
+// TMEM (`tv`), and those passes run warp-uniform trip counts (r.wn) with
+// the lanes whose creature has fewer items idle; otherwise every constant
+// comes from the lane's lines and each lane runs its own trip counts. The
+// arithmetic of an item is the same either way (the *_item functions).
+template <class W, int RATE, bool RECORD, bool TM = false>
 struct Creature {
     using C = Clock<RATE>;
     const W& w;
@@ -40,6 +69,7 @@ struct Creature {
     const Lines& L;
     const SlotLayout& S;
     LaneRegs& r;
+    const TmView* tv = nullptr;
 
     // Joint j from its two lines (shaders/creature.cu:322-356).
     struct Joint {
@@ -210,85 +240,290 @@ struct Creature {
         return make_float2(fx, fy);
     }
 
+    // Air and water drag on bone j (shaders/creature.cu:553-593), from its
+    // lines `ba` (pivot, length, 1/m pivot, 1/m child) and `bb` (air drag
+    // factor, drag limit, the two velocity scales); r0, r1 are the radii of
+    // its two nodes (read only in a world with water).
+    __device__ __forceinline__ void drag_item(unsigned j, const float4& ba, const float4& bb, float r0,
+                                              float r1) const {
+        const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
+        const float2 v0 = t.vel(i0), v1 = t.vel(i1);
+        const float wx = 0.5f * (v0.x + v1.x), wy = 0.5f * (v0.y + v1.y);
+        const float speed = sqrtf(wx * wx + wy * wy);
+        const float limit = bb.y;
+        const float k_air = fminf(bb.x * speed, limit);
+        float dfx = -wx * k_air, dfy = -wy * k_air;
+        if (w.has(CE_FLAG_WATER)) {
+            const float width = r0 + r1;
+            const float2 p0 = t.pos(i0), p1 = t.pos(i1);
+            const float wet0 = clampf((p.water - (p0.y - r0)) / (2.0f * r0), 0.0f, 1.0f);
+            const float wet1 = clampf((p.water - (p1.y - r1)) / (2.0f * r1), 0.0f, 1.0f);
+            const float wet = 0.5f * (wet0 + wet1);
+            const float ax = (p1.x - p0.x) / ba.y, ay = (p1.y - p0.y) / ba.y;
+            const float along = wx * ax + wy * ay;
+            const float lx = ax * along, ly = ay * along;
+            const float sx = wx - lx, sy = wy - ly;
+            const float k_water = fminf(kWaterDrag * wet * ba.y * width * speed, limit);
+            dfx -= sx * k_water + lx * k_water * kWaterAlong;
+            dfy -= sy * k_water + ly * k_water * kWaterAlong;
+        }
+        const float s0 = bb.z, s1 = bb.w;
+        t.vel(i0) = make_float2(v0.x + s0 * dfx, v0.y + s0 * dfy);
+        t.vel(i1) = make_float2(v1.x + s1 * dfx, v1.y + s1 * dfy);
+    }
+
+    // Length of bone j (shaders/creature.cu:597-613).
+    __device__ __forceinline__ void bone_item(unsigned j, const float4& ba) const {
+        const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
+        const float2 p0 = t.pos(i0), p1 = t.pos(i1);
+        const float dx = p1.x - p0.x, dy = p1.y - p0.y;
+        const float len = fmaxf(sqrtf(dx * dx + dy * dy), 1e-9f);
+        const float w0 = ba.z, w1 = ba.w;
+        const float s = (len - ba.y) / ((w0 + w1) * len);
+        t.pos(i0) = make_float2(p0.x + w0 * s * dx, p0.y + w0 * s * dy);
+        t.pos(i1) = make_float2(p1.x - w1 * s * dx, p1.y - w1 * s * dy);
+    }
+
+    // Range of joint j (shaders/creature.cu:618-634).
+    __device__ __forceinline__ void limit_item(unsigned j, const float4& ra, const float4& rb) const {
+        if (__float_as_uint(ra.x) == kNone) {
+            return;
+        }
+        const Joint k = joint(j, ra, rb, true);
+        float error = 0.0f;
+        if (k.angle < k.lo) {
+            error = k.angle - k.lo;
+        }
+        if (k.angle > k.hi) {
+            error = k.angle - k.hi;
+        }
+        if (error == 0.0f) {
+            return;
+        }
+        const float wgt = joint_weight(k);
+        if (wgt > 0.0f) {
+            joint_push<false>(k, -error / wgt);
+        }
+    }
+
+    // Damping of joint j (shaders/creature.cu:683-702).
+    __device__ __forceinline__ void damp_item(unsigned j, const float4& ra, const float4& rb) const {
+        const float share = fminf(C::h * kInvJointDamping, 1.0f);
+        if (__float_as_uint(ra.x) == kNone) {
+            return;
+        }
+        const Joint k = joint(j, ra, rb, false);
+        const float2 vt = t.vel(k.tip), vf = t.vel(k.far), vh = t.vel(k.hub);
+        const float rate = k.g_tip.x * vt.x + k.g_tip.y * vt.y + k.g_far.x * vf.x + k.g_far.y * vf.y +
+                           k.g_hub.x * vh.x + k.g_hub.y * vh.y;
+        const float wgt = joint_weight(k);
+        if (wgt > 0.0f) {
+            joint_push<true>(k, -share * rate / wgt);
+        }
+    }
+
+    // Whether joint j is past its range by more than kJointBreak
+    // (shaders/creature.cu:746-759).
+    __device__ __forceinline__ bool broken_item(unsigned j, const float4& ra, const float4& rb) const {
+        if (__float_as_uint(ra.x) == kNone) {
+            return false;
+        }
+        const Joint k = joint(j, ra, rb, true);
+        return k.angle < k.lo - kJointBreak || k.angle > k.hi + kJointBreak;
+    }
+
+    // World force, muscle force and velocity of node i, then its predicted
+    // position; the force table keeps the start position.
+    __device__ __forceinline__ void integrate_item(unsigned i, const float4& nr) const {
+        const float2 f = node_force(i, nr);
+        float4 s = t.at(i);
+        const float2 fpv = t.f(i);
+        s.z += C::h * (f.x + fpv.x) * nr.y;
+        s.w += C::h * (f.y + fpv.y) * nr.y;
+        if (w.has(CE_FLAG_AIR)) {
+            s.z *= p.air_sub;
+            s.w *= p.air_sub;
+        }
+        t.f(i) = make_float2(s.x, s.y);
+        s.x += C::h * s.z;
+        s.y += C::h * s.w;
+        t.set_at(i, s);
+    }
+
+    // Ground contact of node i, then its velocity from the substep's move.
+    __device__ __forceinline__ void land_item(unsigned i, const float4& nr) const {
+        float2 q = t.pos(i);
+        const float2 f0 = t.f(i);
+        solve_ground(i, nr, q, f0);
+        t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
+    }
+
+    // ------------------------------------------------ TMEM line fetchers
+    // Each fetch issues the loads of one item (TMEM, or the lane's lines for
+    // a kind that does not fit); `wait` makes them usable, after which the
+    // item's lines are assembled in the layout of the lane's lines.
+    struct NodeRaw {
+        float4 q;
+    };
+    __device__ __forceinline__ NodeRaw node_fetch(unsigned i) const {
+        NodeRaw n;
+        n.q = tv->nodes ? tv->tm.ld4(tv->lay.node + 4u * i) : L.get(S.node + i);
+        return n;
+    }
+    __device__ __forceinline__ static void wait(NodeRaw& n) { Tmem::wait(n.q); }
+
+    // Bone j: the quad (pivot, length, 1/m pivot, air factor), 1/m of the
+    // child node, the drag limit and (water) both radii.
+    struct BoneRaw {
+        float4 q;
+        float w1, limit, r0, r1;
+    };
+    template <bool DRAG>
+    __device__ __forceinline__ BoneRaw bone_fetch(unsigned j) const {
+        BoneRaw b;
+        b.limit = b.r0 = b.r1 = 0.0f;
+        if (tv->bones) {
+            b.q = tv->tm.ld4(tv->lay.bone + 4u * j);
+        } else {
+            const float4 ba = L.get(S.bone + 2u * j);
+            b.q = make_float4(ba.x, ba.y, ba.z, DRAG ? L.get(S.bone + 2u * j + 1u).x : 0.0f);
+        }
+        b.w1 = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 1u) : L.get(S.node + j + 1u).y;
+        if (DRAG) {
+            b.limit = tv->limits ? tv->tm.ld1(tv->lay.limit + j) : L.get(S.bone + 2u * j + 1u).y;
+            if (w.has(CE_FLAG_WATER)) {
+                b.r1 = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 2u) : L.get(S.node + j + 1u).z;
+                if (tv->radii) {
+                    b.r0 = tv->tm.ld1(tv->lay.radius + j);
+                }
+            }
+        }
+        return b;
+    }
+    __device__ __forceinline__ static void wait(BoneRaw& b) { Tmem::wait(b.q, b.w1, b.limit, b.r1); }
+    __device__ __forceinline__ float4 bone_a(const BoneRaw& b) const { return make_float4(b.q.x, b.q.y, b.q.z, b.w1); }
+    // The drag scales as the set-up computes them (0.5 h / m).
+    __device__ __forceinline__ float4 bone_b(const BoneRaw& b) const {
+        return make_float4(b.q.w, b.limit, 0.5f * C::h * b.q.z, 0.5f * C::h * b.w1);
+    }
+    __device__ __forceinline__ float bone_r0(const BoneRaw& b) const {
+        if (!w.has(CE_FLAG_WATER)) return 0.0f;
+        return tv->radii ? b.r0 : L.get(S.node + __float_as_uint(b.q.x)).z;
+    }
+
+    // Joint j: the quad (topology, lo, hi, 1/m far node), 1/m of the tip
+    // (node j + 1) and of the hub.
+    struct JointRaw {
+        float4 q;
+        float w_tip, w_hub;
+    };
+    __device__ __forceinline__ JointRaw joint_fetch(unsigned j) const {
+        JointRaw k;
+        if (tv->joints && tv->hubs) {
+            k.q = tv->tm.ld4(tv->lay.joint + 4u * (j - 1u));
+            k.w_hub = tv->tm.ld1(tv->lay.hub + (j - 1u));
+        } else {
+            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            k.q = make_float4(ra.x, ra.y, ra.z, rb.y);
+            k.w_hub = rb.z;
+        }
+        k.w_tip = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 1u) : L.get(S.node + j + 1u).y;
+        return k;
+    }
+    __device__ __forceinline__ static void wait(JointRaw& k) { Tmem::wait(k.q, k.w_tip, k.w_hub); }
+    // The joint's middle angle as the set-up computes it.
+    __device__ __forceinline__ static float4 joint_a(const JointRaw& k) {
+        return make_float4(k.q.x, k.q.y, k.q.z, 0.5f * (k.q.y + k.q.z));
+    }
+    __device__ __forceinline__ static float4 joint_b(const JointRaw& k) {
+        return make_float4(k.w_tip, k.q.w, k.w_hub, 0.0f);
+    }
+
+    // A warp-uniform pass over items first .. last - 1 with the next item's
+    // loads in flight while the current one is worked on. `work(j, raw)`
+    // runs on the lanes whose creature has item j (`has(j)`).
+    template <class Raw, class Fetch, class Has, class Work>
+    __device__ __forceinline__ void tm_pass(unsigned first, unsigned last, Fetch fetch, Has has,
+                                            Work work) const {
+        if (first >= last) {
+            return;
+        }
+        __syncwarp();  // lanes may arrive from loops of their own lengths
+        Raw cur = fetch(first);
+        wait(cur);
+        for (unsigned j = first; j < last; j++) {
+            const unsigned nj = j + 1u < last ? j + 1u : j;
+            Raw nxt = fetch(nj);
+            if (has(j)) {
+                work(j, cur);
+            }
+            __syncwarp();  // the TMEM wait and the next loads are warp-wide
+            wait(nxt);
+            cur = nxt;
+        }
+    }
+
+    // ------------------------------------------------------------ passes
     // Air and water drag on the bones (shaders/creature.cu:553-593).
     __device__ __forceinline__ void bone_drag() const {
-        const unsigned bones = r.nodes - 1u;
-        float4 na = L.get(S.bone), nb = L.get(S.bone + 1u);
-        for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = na, bb = nb;
-            na = L.get(S.bone + 2u * j + 2u);
-            nb = L.get(S.bone + 2u * j + 3u);
-            const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
-            const float2 v0 = t.vel(i0), v1 = t.vel(i1);
-            const float wx = 0.5f * (v0.x + v1.x), wy = 0.5f * (v0.y + v1.y);
-            const float speed = sqrtf(wx * wx + wy * wy);
-            const float limit = bb.y;
-            const float k_air = fminf(bb.x * speed, limit);
-            float dfx = -wx * k_air, dfy = -wy * k_air;
-            if (w.has(CE_FLAG_WATER)) {
-                const float r0 = L.get(S.node + i0).z, r1 = L.get(S.node + i1).z;
-                const float width = r0 + r1;
-                const float2 p0 = t.pos(i0), p1 = t.pos(i1);
-                const float wet0 = clampf((p.water - (p0.y - r0)) / (2.0f * r0), 0.0f, 1.0f);
-                const float wet1 = clampf((p.water - (p1.y - r1)) / (2.0f * r1), 0.0f, 1.0f);
-                const float wet = 0.5f * (wet0 + wet1);
-                const float ax = (p1.x - p0.x) / ba.y, ay = (p1.y - p0.y) / ba.y;
-                const float along = wx * ax + wy * ay;
-                const float lx = ax * along, ly = ay * along;
-                const float sx = wx - lx, sy = wy - ly;
-                const float k_water = fminf(kWaterDrag * wet * ba.y * width * speed, limit);
-                dfx -= sx * k_water + lx * k_water * kWaterAlong;
-                dfy -= sy * k_water + ly * k_water * kWaterAlong;
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<BoneRaw>(
+                0u, r.wn > 0u ? r.wn - 1u : 0u, [&](unsigned j) { return bone_fetch<true>(j); },
+                [&](unsigned j) { return j + 1u < nodes; },
+                [&](unsigned j, const BoneRaw& b) { drag_item(j, bone_a(b), bone_b(b), bone_r0(b), b.r1); });
+        } else {
+            const unsigned bones = r.nodes - 1u;
+            float4 na = L.get(S.bone), nb = L.get(S.bone + 1u);
+            for (unsigned j = 0u; j < bones; j++) {
+                const float4 ba = na, bb = nb;
+                na = L.get(S.bone + 2u * j + 2u);
+                nb = L.get(S.bone + 2u * j + 3u);
+                float r0 = 0.0f, r1 = 0.0f;
+                if (w.has(CE_FLAG_WATER)) {
+                    r0 = L.get(S.node + __float_as_uint(ba.x)).z;
+                    r1 = L.get(S.node + j + 1u).z;
+                }
+                drag_item(j, ba, bb, r0, r1);
             }
-            const float s0 = bb.z, s1 = bb.w;
-            t.vel(i0) = make_float2(v0.x + s0 * dfx, v0.y + s0 * dfy);
-            t.vel(i1) = make_float2(v1.x + s1 * dfx, v1.y + s1 * dfy);
         }
     }
 
     // Bone lengths (shaders/creature.cu:597-613).
     __device__ __forceinline__ void solve_bones() const {
-        const unsigned bones = r.nodes - 1u;
-        float4 na = L.get(S.bone);
-        for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = na;
-            na = L.get(S.bone + 2u * j + 2u);
-            const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
-            const float2 p0 = t.pos(i0), p1 = t.pos(i1);
-            const float dx = p1.x - p0.x, dy = p1.y - p0.y;
-            const float len = fmaxf(sqrtf(dx * dx + dy * dy), 1e-9f);
-            const float w0 = ba.z, w1 = ba.w;
-            const float s = (len - ba.y) / ((w0 + w1) * len);
-            t.pos(i0) = make_float2(p0.x + w0 * s * dx, p0.y + w0 * s * dy);
-            t.pos(i1) = make_float2(p1.x - w1 * s * dx, p1.y - w1 * s * dy);
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<BoneRaw>(
+                0u, r.wn > 0u ? r.wn - 1u : 0u, [&](unsigned j) { return bone_fetch<false>(j); },
+                [&](unsigned j) { return j + 1u < nodes; },
+                [&](unsigned j, const BoneRaw& b) { bone_item(j, bone_a(b)); });
+        } else {
+            const unsigned bones = r.nodes - 1u;
+            float4 na = L.get(S.bone);
+            for (unsigned j = 0u; j < bones; j++) {
+                const float4 ba = na;
+                na = L.get(S.bone + 2u * j + 2u);
+                bone_item(j, ba);
+            }
         }
     }
 
     // Joint ranges (shaders/creature.cu:618-634).
     __device__ __forceinline__ void solve_joints() const {
-        const unsigned bones = r.nodes - 1u;
-        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-        for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = na, rb = nb;
-            na = L.get(S.joint + 2u * j + 2u);
-            nb = L.get(S.joint + 2u * j + 3u);
-            if (__float_as_uint(ra.x) == kNone) {
-                continue;
-            }
-            const Joint k = joint(j, ra, rb, true);
-            float error = 0.0f;
-            if (k.angle < k.lo) {
-                error = k.angle - k.lo;
-            }
-            if (k.angle > k.hi) {
-                error = k.angle - k.hi;
-            }
-            if (error == 0.0f) {
-                continue;
-            }
-            const float wgt = joint_weight(k);
-            if (wgt > 0.0f) {
-                joint_push<false>(k, -error / wgt);
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<JointRaw>(
+                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
+                [&](unsigned j) { return j + 1u < nodes; },
+                [&](unsigned j, const JointRaw& k) { limit_item(j, joint_a(k), joint_b(k)); });
+        } else {
+            const unsigned bones = r.nodes - 1u;
+            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
+            for (unsigned j = 1u; j < bones; j++) {
+                const float4 ra = na, rb = nb;
+                na = L.get(S.joint + 2u * j + 2u);
+                nb = L.get(S.joint + 2u * j + 3u);
+                limit_item(j, ra, rb);
             }
         }
     }
@@ -338,23 +573,49 @@ struct Creature {
 
     // Joint damping (shaders/creature.cu:683-702).
     __device__ __forceinline__ void damp_joints() const {
-        const float share = fminf(C::h * kInvJointDamping, 1.0f);
-        const unsigned bones = r.nodes - 1u;
-        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-        for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = na, rb = nb;
-            na = L.get(S.joint + 2u * j + 2u);
-            nb = L.get(S.joint + 2u * j + 3u);
-            if (__float_as_uint(ra.x) == kNone) {
-                continue;
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<JointRaw>(
+                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
+                [&](unsigned j) { return j + 1u < nodes; },
+                [&](unsigned j, const JointRaw& k) { damp_item(j, joint_a(k), joint_b(k)); });
+        } else {
+            const unsigned bones = r.nodes - 1u;
+            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
+            for (unsigned j = 1u; j < bones; j++) {
+                const float4 ra = na, rb = nb;
+                na = L.get(S.joint + 2u * j + 2u);
+                nb = L.get(S.joint + 2u * j + 3u);
+                damp_item(j, ra, rb);
             }
-            const Joint k = joint(j, ra, rb, false);
-            const float2 vt = t.vel(k.tip), vf = t.vel(k.far), vh = t.vel(k.hub);
-            const float rate = k.g_tip.x * vt.x + k.g_tip.y * vt.y + k.g_far.x * vf.x + k.g_far.y * vf.y +
-                               k.g_hub.x * vh.x + k.g_hub.y * vh.y;
-            const float wgt = joint_weight(k);
-            if (wgt > 0.0f) {
-                joint_push<true>(k, -share * rate / wgt);
+        }
+    }
+
+    // The per-node passes of a substep: `LAND` false integrates forces,
+    // true does ground contact and velocities.
+    template <bool LAND>
+    __device__ __forceinline__ void node_pass() const {
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<NodeRaw>(
+                0u, r.wn, [&](unsigned i) { return node_fetch(i); }, [&](unsigned i) { return i < nodes; },
+                [&](unsigned i, const NodeRaw& n) {
+                    if (LAND) {
+                        land_item(i, n.q);
+                    } else {
+                        integrate_item(i, n.q);
+                    }
+                });
+        } else {
+            float4 nn = L.get(S.node);
+            for (unsigned i = 0u; i < r.nodes; i++) {
+                const float4 nr = nn;
+                nn = L.get(S.node + i + 1u);
+                if (LAND) {
+                    land_item(i, nr);
+                } else {
+                    integrate_item(i, nr);
+                }
             }
         }
     }
@@ -363,35 +624,10 @@ struct Creature {
     __device__ __forceinline__ void substep() const {
         muscle_forces();
         bone_drag();
-        float4 nn = L.get(S.node);
-        for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = nn;
-            nn = L.get(S.node + i + 1u);
-            const float2 f = node_force(i, nr);
-            float4 s = t.at(i);
-            const float2 fpv = t.f(i);
-            s.z += C::h * (f.x + fpv.x) * nr.y;
-            s.w += C::h * (f.y + fpv.y) * nr.y;
-            if (w.has(CE_FLAG_AIR)) {
-                s.z *= p.air_sub;
-                s.w *= p.air_sub;
-            }
-            t.f(i) = make_float2(s.x, s.y);
-            s.x += C::h * s.z;
-            s.y += C::h * s.w;
-            t.set_at(i, s);
-        }
+        node_pass<false>();
         solve_bones();
         solve_joints();
-        nn = L.get(S.node);
-        for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = nn;
-            nn = L.get(S.node + i + 1u);
-            float2 q = t.pos(i);
-            const float2 f0 = t.f(i);
-            solve_ground(i, nr, q, f0);
-            t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
-        }
+        node_pass<true>();
         damp_joints();
     }
 
@@ -399,18 +635,26 @@ struct Creature {
     // (shaders/creature.cu:746-759).
     __device__ __forceinline__ unsigned long long broken_joints() const {
         unsigned long long bits = 0ull;
-        const unsigned bones = r.nodes - 1u;
-        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-        for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = na, rb = nb;
-            na = L.get(S.joint + 2u * j + 2u);
-            nb = L.get(S.joint + 2u * j + 3u);
-            if (__float_as_uint(ra.x) == kNone) {
-                continue;
-            }
-            const Joint k = joint(j, ra, rb, true);
-            if (k.angle < k.lo - kJointBreak || k.angle > k.hi + kJointBreak) {
-                bits |= 1ull << j;
+        if constexpr (TM) {
+            const unsigned nodes = r.nodes;
+            tm_pass<JointRaw>(
+                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
+                [&](unsigned j) { return j + 1u < nodes; },
+                [&](unsigned j, const JointRaw& k) {
+                    if (broken_item(j, joint_a(k), joint_b(k))) {
+                        bits |= 1ull << j;
+                    }
+                });
+        } else {
+            const unsigned bones = r.nodes - 1u;
+            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
+            for (unsigned j = 1u; j < bones; j++) {
+                const float4 ra = na, rb = nb;
+                na = L.get(S.joint + 2u * j + 2u);
+                nb = L.get(S.joint + 2u * j + 3u);
+                if (broken_item(j, ra, rb)) {
+                    bits |= 1ull << j;
+                }
             }
         }
         return bits;

@@ -122,7 +122,7 @@ struct ce_engine {
     uint32_t fault_after = 0;
     ce_status fault_status = CE_OK;
     // Recording buffers.
-    DeviceBuf rec_frames, rec_lanes, rec_muscles, rec_heads, rec_results, rec_counter, rec_scratch;
+    DeviceBuf rec_frames, rec_staging, rec_lanes, rec_muscles, rec_heads, rec_results, rec_counter, rec_scratch;
 };
 
 namespace {
@@ -162,8 +162,12 @@ size_t scratch_bytes(unsigned grid, unsigned rows, unsigned mm, bool record) {
 // 2.51 s against 2.77 s one class after the other; at 8 (work 1.12) 4.32 s
 // against 2.96 s; at 10 (0.65) 3.91 s against 2.81 s; at 16 (0.17, 1 small
 // block of 3) 3.87 s against 2.91 s.
-std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& plans, uint32_t flags, int rate) {
+// `shares` receives, per class, how many creature-kernel blocks may share a
+// multiprocessor while it runs (0: its own occupancy), which splits TMEM.
+std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& plans, uint32_t flags, int rate,
+                                  std::vector<unsigned>* shares = nullptr) {
     std::vector<unsigned> grids(plans.size());
+    if (shares) shares->assign(plans.size(), 0u);
     for (size_t c = 0; c < plans.size(); c++) {
         grids[c] = grid_for(e, plans[c].rows, plans[c].mm, flags, false, rate, plans[c].count);
     }
@@ -185,6 +189,7 @@ std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& pl
     if (2u * small_per_sm < (unsigned)alone_small) return grids;
     grids[0] = std::min<unsigned>(grids[0], small_per_sm * (unsigned)e->sms);
     grids[1] = std::min<unsigned>(grids[1], (unsigned)e->sms);
+    if (shares) shares->assign(2, small_per_sm + 1u);
     return grids;
 }
 
@@ -357,6 +362,7 @@ extern "C" ce_status ce_close(ce_engine* e) {
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     e->rec_frames.release();
+    e->rec_staging.release();
     e->rec_lanes.release();
     e->rec_muscles.release();
     e->rec_heads.release();
@@ -376,7 +382,7 @@ extern "C" int ce_free_slots(ce_engine* e) {
 
 extern "C" size_t ce_allocated_bytes(ce_engine* e) {
     if (!e) return 0;
-    size_t b = e->rec_frames.bytes + e->rec_lanes.bytes + e->rec_muscles.bytes + e->rec_heads.bytes +
+    size_t b = e->rec_frames.bytes + e->rec_staging.bytes + e->rec_lanes.bytes + e->rec_muscles.bytes + e->rec_heads.bytes +
                e->rec_results.bytes + e->rec_counter.bytes + e->rec_scratch.bytes;
     for (const Slot& sl : e->slots) {
         b += sl.d_lanes.bytes + sl.d_muscles.bytes + sl.d_heads.bytes + sl.d_results.bytes + sl.d_buckets.bytes +
@@ -443,7 +449,8 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     ce_make_params(w, 0, (uint32_t)pack->count, 0, &p);
     // Grids and scratch of the classes, which run side by side, each with its
     // own part of the slot's scratch.
-    const std::vector<unsigned> grids = class_grids(e, plans, flags, rate);
+    std::vector<unsigned> shares;
+    const std::vector<unsigned> grids = class_grids(e, plans, flags, rate, &shares);
     std::vector<size_t> scratch_at(plans.size());
     size_t scratch = 0;
     for (size_t c = 0; c < plans.size(); c++) {
@@ -489,7 +496,7 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
         a.frames_per_creature = 0;
         a.chunk_k = e->chunk_k;
         cek::LaunchSpec ls{plans[c].rows, plans[c].mm, flags, false, rate, grids[c], cek::kBlock,
-                           c == 0 ? st : sl.side};
+                           c == 0 ? st : sl.side, shares[c]};
         CE_TRY(cek::launch_advance(ls, a, p), "advance launch");
     }
     CE_TRY(cudaEventRecord(sl.joined, sl.side), "cudaEventRecord");
@@ -601,7 +608,8 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     const unsigned grid = grid_for(e, rows, mm, flags, true, rate, pack->count);
     const size_t lanes_b = pack->lanes_len * 4, mus_b = pack->muscles_len * 4, heads_b = pack->count * 32;
     const size_t res_b = pack->count * sizeof(ce_result);
-    if ((s = e->rec_frames.ensure(frame_floats * 4)) || (s = e->rec_lanes.ensure(lanes_b)) ||
+    if ((s = e->rec_frames.ensure(frame_floats * 4)) || (s = e->rec_staging.ensure(frame_floats * 4)) ||
+        (s = e->rec_lanes.ensure(lanes_b)) ||
         (s = e->rec_muscles.ensure(mus_b)) || (s = e->rec_heads.ensure(heads_b)) || (s = e->rec_results.ensure(res_b)) ||
         (s = e->rec_counter.ensure(4)) || (s = e->rec_scratch.ensure(scratch_bytes(grid, rows, mm, true)))) {
         return s;
@@ -610,7 +618,7 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     CE_TRY(cudaMemcpy(e->rec_muscles.ptr, pack->muscles, mus_b, cudaMemcpyHostToDevice), "cudaMemcpy");
     CE_TRY(cudaMemcpy(e->rec_heads.ptr, pack->heads, heads_b, cudaMemcpyHostToDevice), "cudaMemcpy");
     CE_TRY(cudaMemset(e->rec_counter.ptr, 0, 4), "cudaMemset");
-    CE_TRY(cudaMemset(e->rec_frames.ptr, 0, frame_floats * 4), "cudaMemset");
+    CE_TRY(cudaMemset(e->rec_staging.ptr, 0, frame_floats * 4), "cudaMemset");
     cek::KernelArgs a{};
     a.records = static_cast<const uint32_t*>(e->rec_lanes.ptr);
     a.muscles = static_cast<const float*>(e->rec_muscles.ptr);
@@ -618,7 +626,7 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     a.results = static_cast<ce_result*>(e->rec_results.ptr);
     a.counter = static_cast<uint32_t*>(e->rec_counter.ptr);
     a.scratch = static_cast<float4*>(e->rec_scratch.ptr);
-    a.frames = static_cast<float2*>(e->rec_frames.ptr);
+    a.frames = static_cast<float2*>(e->rec_staging.ptr);
     a.order = nullptr;
     a.count = (uint32_t)pack->count;
     a.rows = rows;
@@ -627,6 +635,10 @@ extern "C" ce_status ce_record(ce_engine* e, const ce_wave_pack* pack, const ce_
     a.chunk_k = 1;
     cek::LaunchSpec ls{rows, mm, flags, true, rate, grid, cek::kBlock, nullptr};
     CE_TRY(cek::launch_advance(ls, a, p), "record launch");
+    CE_TRY(cek::launch_frames_to_creature_major(static_cast<const float2*>(e->rec_staging.ptr),
+                                                static_cast<float2*>(e->rec_frames.ptr), (size_t)per * stride,
+                                                (uint32_t)pack->count, nullptr),
+           "frame transpose launch");
     CE_TRY(cudaDeviceSynchronize(), "record kernel");
     CE_TRY(cudaMemcpy(frames, e->rec_frames.ptr, frame_floats * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
     CE_TRY(cudaMemcpy(results, e->rec_results.ptr, res_b, cudaMemcpyDeviceToHost), "cudaMemcpy");
@@ -649,17 +661,20 @@ extern "C" size_t ce_advance_scratch_bytes(ce_engine* e, uint32_t world_flags, u
     return slots_part(e, world_flags, rate, max_nodes, max_muscles) + cek::bucket_bytes(count);
 }
 
-extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, const float* muscles,
-                                       const uint32_t* heads, ce_result* results, uint32_t* counter, void* scratch,
-                                       const ce_params* params, uint32_t world_flags, uint32_t rate,
-                                       uint32_t max_nodes, uint32_t max_muscles, void* stream) {
+namespace {
+// The device entry, with the niche epilogue when `cells` is given.
+ce_status advance_device(ce_engine* e, const uint32_t* records, const float* muscles, const uint32_t* heads,
+                         ce_result* results, uint32_t* counter, void* scratch, const ce_params* params,
+                         uint32_t world_flags, uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
+                         void* stream, const uint8_t* shapes, const cek::MetricsArgs* niche, ce_metrics* metrics,
+                         int64_t* cells, const char* what) {
     if (!e || !records || !muscles || !heads || !results || !counter || !scratch || !params) {
-        set_error("ce_advance_device: null argument");
+        set_error(std::string(what) + ": null argument");
         return CE_ERR_INVALID;
     }
     if (max_nodes < 2 || max_nodes > CE_MAX_NODES || max_muscles > CE_MAX_MUSCLES || params->steps < 1 ||
         (rate != 60 && rate != 120)) {
-        set_error("ce_advance_device: unsupported sizes");
+        set_error(std::string(what) + ": unsupported sizes");
         return CE_ERR_INVALID;
     }
     CE_TRY(cudaSetDevice(e->device), "cudaSetDevice");
@@ -686,9 +701,41 @@ extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, co
     a.mm = max_muscles;
     a.frames_per_creature = 0;
     a.chunk_k = e->chunk_k;
+    if (cells) {
+        a.shapes = shapes;
+        a.metrics = metrics;
+        a.cells = cells;
+        a.niche = *niche;
+    }
     cek::LaunchSpec ls{max_nodes, max_muscles, world_flags, false, (int)rate, grid, cek::kBlock, st};
     CE_TRY(cek::launch_advance(ls, a, *params), "advance launch");
     return CE_OK;
+}
+}  // namespace
+
+extern "C" ce_status ce_advance_device(ce_engine* e, const uint32_t* records, const float* muscles,
+                                       const uint32_t* heads, ce_result* results, uint32_t* counter, void* scratch,
+                                       const ce_params* params, uint32_t world_flags, uint32_t rate,
+                                       uint32_t max_nodes, uint32_t max_muscles, void* stream) {
+    return advance_device(e, records, muscles, heads, results, counter, scratch, params, world_flags, rate,
+                          max_nodes, max_muscles, stream, nullptr, nullptr, nullptr, nullptr, "ce_advance_device");
+}
+
+extern "C" ce_status ce_advance_device_cells(ce_engine* e, const uint32_t* records, const float* muscles,
+                                             const uint32_t* heads, ce_result* results, uint32_t* counter,
+                                             void* scratch, const ce_params* params, const ce_world* world,
+                                             uint32_t max_nodes, uint32_t max_muscles, const uint8_t* shape_classes,
+                                             int global_layout, ce_metrics* metrics, int64_t* cells, void* stream) {
+    if (!world || !shape_classes || !cells) {
+        set_error("ce_advance_device_cells: null argument");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = check_world(world);
+    if (s != CE_OK) return s;
+    const cek::MetricsArgs k = cek::metrics_args(world, global_layout);
+    return advance_device(e, records, muscles, heads, results, counter, scratch, params, ce_world_flags(world),
+                          ce::world_rate(*world), max_nodes, max_muscles, stream, shape_classes, &k, metrics, cells,
+                          "ce_advance_device_cells");
 }
 
 // ------------------------------------------------------------- gradients
@@ -1014,7 +1061,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
     ce_params p;
     // Plans, grids and scratch of every generation; one scratch a class.
     std::vector<std::vector<ClassPlan>> plans(generations);
-    std::vector<std::vector<unsigned>> grids(generations);
+    std::vector<std::vector<unsigned>> grids(generations), shares(generations);
     size_t scratch_need[2] = {0, 0};
     g->gens.resize(generations);
     for (uint32_t k = 0; k < generations; k++) {
@@ -1024,7 +1071,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
             return fail(CE_ERR_INVALID);
         }
         if ((s = plan_classes(pack, plans[k], e->small_body)) != CE_OK) return fail(s);
-        const std::vector<unsigned> kg = class_grids(e, plans[k], flags, rate);
+        const std::vector<unsigned> kg = class_grids(e, plans[k], flags, rate, &shares[k]);
         for (size_t ci = 0; ci < plans[k].size(); ci++) {
             const ClassPlan& c = plans[k][ci];
             const unsigned grid = kg[ci];
@@ -1085,7 +1132,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
             a.mm = plans[k][c].mm;
             a.chunk_k = e->chunk_k;
             cek::LaunchSpec ls{plans[k][c].rows, plans[k][c].mm, flags, false, rate, grids[k][c], cek::kBlock,
-                               c == 0 ? g->stream : g->side};
+                               c == 0 ? g->stream : g->side, shares[k][c]};
             cap = cuda_status(cek::launch_advance(ls, a, p), "advance launch");
         }
         if (cap == CE_OK) cap = cuda_status(cudaEventRecord(g->events[2 * k + 1], g->side), "cudaEventRecord");

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "../../include/creature_engine.h"
+#include "niche.cuh"
 
 namespace cek {
 
@@ -60,7 +61,18 @@ struct KernelArgs {
     float* ckpt;                   // CKPT: checkpoints, ckpt_stride floats a creature (packed index)
     uint32_t ckpt_stride;
     uint32_t* ends;                // CKPT: steps each creature's trial ran (packed index)
+    uint32_t tmem_cols;            // plain kernel: TMEM columns a block allocates (tmem.cuh)
+    // Niche epilogue at the result store (plain kernel; `cells` NULL: none):
+    // each creature's metrics row (`metrics` may be NULL) and dense cell,
+    // from its result, node count and shape class (packed index).
+    const uint8_t* shapes;
+    ce_metrics* metrics;
+    int64_t* cells;
+    MetricsArgs niche;
 };
+
+// Metrics arguments of a world in the global (1) or an island's (0) layout.
+MetricsArgs metrics_args(const ce_world* world, int global_layout);
 
 // Floats of one checkpoint: positions and velocities of `rows` nodes, then
 // the energy stores of `mm` muscles.
@@ -113,12 +125,21 @@ struct LaunchSpec {
     int rate;        // steps per second: 60 or 120
     unsigned grid, block;
     cudaStream_t stream;
+    // Blocks of creature kernels that may share a multiprocessor while this
+    // launch runs (its own and another launch's beside it), which splits the
+    // 512 TMEM columns; 0: this launch's own occupancy.
+    unsigned sm_share = 0;
 };
 
 // 16-byte lines of one lane's slot.
 unsigned slot_lines(unsigned rows, unsigned mm, bool record);
 
 cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
+// A recording's frames from the kernel's frame-major, creature-minor layout
+// (`rows` = frames x slots rows of `creatures` entries) to the reference's
+// creature-major one (`creatures` rows of `rows` entries).
+cudaError_t launch_frames_to_creature_major(const float2* src, float2* dst, size_t rows, uint32_t creatures,
+                                            cudaStream_t stream);
 cudaError_t advance_occupancy(unsigned rows, unsigned mm, uint32_t flags, bool record, int rate, unsigned block,
                               int* blocks);
 // Sets the kernel's dynamic shared-memory limit for `rows` x `mm` tables: a

@@ -1,14 +1,8 @@
 // The metrics epilogue on the device: scheduler::to_metrics
 // (src/scheduler.rs:859-923) and Descriptor::niche_in with cell_index
 // (src/qd.rs:762-846, 988-999) for every result of a batch, so the archive
-// gets its cells without a host pass over the results.
-//
-// Cells must equal the host's to the bit. The arithmetic is the host's with
-// every rounding explicit (IEEE division, no fused multiply-add); the height
-// axis, a logarithm on the host, becomes a comparison with the five heights
-// where its bin steps up, which the host finds with its own arithmetic
-// (height_bin_thresholds); a body's shape class depends on its genes alone
-// and comes computed per creature (ce_shape_classes).
+// gets its cells without a host pass over the results (niche.cuh holds the
+// arithmetic, which the creature kernel also runs at its result store).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,65 +12,15 @@
 
 #include "../../include/creature_engine.h"
 #include "host_model.h"
+#include "kernels.h"
+#include "niche.cuh"
+
+using cek::Behavior;
+using cek::MetricsArgs;
+using cek::behavior;
+using cek::to_metrics;
 
 namespace {
-
-struct MetricsArgs {
-    uint32_t all_steps;
-    float rate;
-    float height_edges[5];
-    uint32_t node_edges[3];
-    uint32_t edges;  // 3 for the global layout, 2 for an island's
-};
-
-__device__ __forceinline__ float clamp_host(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
-
-__device__ __forceinline__ uint32_t qd_bin(float v, float lo, float hi, uint32_t count) {
-    const float f = floorf(__fmul_rn(__fdiv_rn(__fsub_rn(clamp_host(v, lo, hi), lo), __fsub_rn(hi, lo)), (float)count));
-    const uint32_t b = f <= 0.0f ? 0u : (f >= 255.0f ? 255u : (uint32_t)f);
-    return min(b, count - 1u);
-}
-
-// scheduler::to_metrics of one result of a body with `nodes` nodes.
-__device__ __forceinline__ ce_metrics to_metrics(const ce_result& r, uint32_t nodes, const MetricsArgs& k) {
-    const float ended = r.fall_time > 0.0f ? r.fall_time : r.screened;
-    uint32_t steps = k.all_steps;
-    if (ended > 0.0f) {
-        const float x = roundf(__fmul_rn(ended, k.rate));
-        const uint32_t s = x <= 0.0f ? 0u : (x >= 4294967295.0f ? 0xffffffffu : (uint32_t)x);
-        steps = min(max(s, 1u), k.all_steps);
-    }
-    const float denom = (float)(steps * nodes);
-    ce_metrics m;
-    m.fitness = r.fitness;
-    m.ground_contact = clamp_host(__fdiv_rn(r.ground_contact, denom), 0.0f, 1.0f);
-    m.vertical_oscillation = isfinite(r.vertical_oscillation) ? fmaxf(r.vertical_oscillation, 0.0f) : 0.0f;
-    m.gait_frequency = isfinite(r.gait_frequency) ? fmaxf(r.gait_frequency, 0.0f) : 0.0f;
-    m.mean_height = fmaxf(__fdiv_rn(r.height_sum, (float)steps), 0.0f);
-    m.feet = (float)__popc(__float_as_uint(r.lift_lo));
-    m.screen_x = r.screen_x;
-    m.screened = r.screened > 0.0f ? 1u : 0u;
-    m.steps = steps;
-    return m;
-}
-
-// The behaviour axes of a niche (Descriptor::niche_in, src/qd.rs:795-806):
-// contact, cadence, height and feet (the last one less 1).
-struct Behavior {
-    uint32_t gc, gf, hb, feet;
-};
-__device__ __forceinline__ Behavior behavior(const ce_metrics& m, const MetricsArgs& k) {
-    Behavior v;
-    v.gc = qd_bin(clamp_host(m.ground_contact, 0.0f, 1.0f), 0.0f, 1.0f, 6u);
-    v.gf = qd_bin(clamp_host(m.gait_frequency, 0.0f, 20.0f), 0.0f, 6.0f, 8u);
-    const float mh = fmaxf(m.mean_height, 0.0f);
-    v.hb = 0u;
-    for (int b = 0; b < 5; b++) v.hb += mh >= k.height_edges[b] ? 1u : 0u;
-    const float fr = roundf(fmaxf(m.feet, 0.0f));
-    int fi = fr >= 2147483647.0f ? 2147483647 : (fr <= -2147483648.0f ? (-2147483647 - 1) : (int)fr);
-    v.feet = (uint32_t)(min(max(fi, 1), 5) - 1);
-    return v;
-}
 
 __global__ void metrics_kernel(const ce_result* results, const uint4* heads, const uint8_t* shape, size_t count,
                                const MetricsArgs k, ce_metrics* metrics, int64_t* cells) {
@@ -85,19 +29,7 @@ __global__ void metrics_kernel(const ce_result* results, const uint4* heads, con
         const uint32_t nodes = heads[2 * c].x & 255u;
         const ce_metrics m = to_metrics(r, nodes, k);
         if (metrics) metrics[c] = m;
-        const Behavior v = behavior(m, k);
-        const uint32_t gc = v.gc, gf = v.gf, hb = v.hb;
-        const int fi = (int)v.feet + 1;
-        uint32_t size = 0u;
-        for (uint32_t e = 0; e < k.edges; e++) size += nodes >= k.node_edges[e] ? 1u : 0u;
-        const uint32_t classes = k.edges + 1u;
-        const uint32_t sh = shape[c];
-        int64_t index = -1;
-        if (sh < classes) {
-            index = ((((int64_t)gc * 8 + gf) * classes + sh) * 6 + hb) * 5 + (fi - 1);
-            index = index * classes + size;
-        }
-        cells[c] = index;
+        cells[c] = cek::cell_of(m, nodes, shape[c], k);
     }
 }
 
@@ -140,6 +72,9 @@ __global__ void dump_rows_kernel(const ce_result* results, const uint4* heads, c
     }
 }
 
+}  // namespace
+
+namespace cek {
 MetricsArgs metrics_args(const ce_world* world, int global_layout) {
     MetricsArgs k;
     k.all_steps = std::max(ce::world_steps(*world), 1u);
@@ -158,8 +93,9 @@ MetricsArgs metrics_args(const ce_world* world, int global_layout) {
     }
     return k;
 }
+}  // namespace cek
 
-}  // namespace
+using cek::metrics_args;
 
 // Metrics and dense cells of `count` results on the device (device
 // pointers; `metrics` may be NULL); asynchronous on `stream`.

@@ -11,27 +11,36 @@ namespace cek {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-template <class W, bool RECORD, int RATE, bool CKPT = false>
+// TM: the creature's node, bone and joint constants come from TMEM (only
+// for the plain kernel, neither recording nor checkpointing); step() is then
+// called by every lane of the warp, `live` telling whether its lane has a
+// creature, since the passes' TMEM loads are warp-wide.
+template <class W, bool RECORD, int RATE, bool CKPT = false, bool TM = false>
 struct Trial {
+    static_assert(!(TM && (RECORD || CKPT)), "TMEM constants are for the plain kernel");
     using C = Clock<RATE>;
-    using Body = Creature<W, RATE, RECORD>;
+    using Body = Creature<W, RATE, RECORD, TM>;
 
-    // Frame t of a recording (shaders/creature.cu:767-779), in the
-    // reference's frame layout.
+    // Frame t of a recording (shaders/creature.cu:767-779): the reference's
+    // frame slots, stored frame-major and creature-minor (slot s of frame t
+    // of recorded creature c at (t * stride + s) * count + c), so the lanes
+    // of a warp, which record consecutive creatures in step with each other,
+    // store each slot as one coalesced run. frames_to_creature_major turns
+    // them into the reference's creature-major layout.
     __device__ __forceinline__ static void record_frame(const Body& b, const KernelArgs& a, unsigned t) {
         const unsigned stride = b.p.stride;
-        float2* fr = a.frames + ((size_t)b.r.rec_slot * a.frames_per_creature + t) * stride;
+        const size_t k = a.count;
+        float2* fr = a.frames + (size_t)t * stride * k + b.r.rec_slot;
         for (unsigned i = 0u; i < b.r.nodes; i++) {
             const float4 fl = b.L.get(b.S.rec_force + i);
-            fr[i] = b.t.pos(i);
-            fr[CE_MAX_NODES + b.r.muscles + i] = make_float2(fl.x, fl.y);
+            fr[i * k] = b.t.pos(i);
+            fr[(CE_MAX_NODES + b.r.muscles + i) * k] = make_float2(fl.x, fl.y);
         }
-        for (unsigned k = 0u; k < b.r.muscles; k++) {
-            fr[CE_MAX_NODES + k] =
-                make_float2(b.t.muscle(k).x, b.L.word(b.S.rec_pull + k / 4u, k % 4u));
+        for (unsigned m = 0u; m < b.r.muscles; m++) {
+            fr[(CE_MAX_NODES + m) * k] = make_float2(b.t.muscle(m).x, b.L.word(b.S.rec_pull + m / 4u, m % 4u));
         }
         const unsigned long long broken = b.broken_joints();
-        fr[stride - 1u] =
+        fr[(stride - 1u) * k] =
             make_float2(__uint_as_float((unsigned)broken), __uint_as_float((unsigned)(broken >> 32)));
     }
 
@@ -154,9 +163,114 @@ struct Trial {
         }
     }
 
+    // Word `c` of the TMEM layout of this lane's creature, from the lines
+    // that begin() wrote (TmLayout: the same values, laid out for TMEM).
+    __device__ __forceinline__ static float tm_word(const Body& b, const TmLayout& lay, unsigned c) {
+        const Lines& L = b.L;
+        const SlotLayout& S = b.S;
+        if (c < lay.bone) {
+            const float4 v = L.get(S.node + c / 4u);
+            const unsigned k = c % 4u;
+            return k == 0u ? v.x : k == 1u ? v.y : k == 2u ? v.z : v.w;
+        }
+        if (c < lay.joint) {
+            const unsigned j = (c - lay.bone) / 4u, k = (c - lay.bone) % 4u;
+            if (k == 3u) return L.get(S.bone + 2u * j + 1u).x;
+            const float4 v = L.get(S.bone + 2u * j);
+            return k == 0u ? v.x : k == 1u ? v.y : v.z;
+        }
+        if (c < lay.limit) {
+            const unsigned j = 1u + (c - lay.joint) / 4u, k = (c - lay.joint) % 4u;
+            if (k == 3u) return L.get(S.joint + 2u * j + 1u).y;
+            const float4 v = L.get(S.joint + 2u * j);
+            return k == 0u ? v.x : k == 1u ? v.y : v.z;
+        }
+        if (c < lay.hub) {
+            return L.get(S.bone + 2u * (c - lay.limit) + 1u).y;
+        }
+        if (c < lay.radius) {
+            return L.get(S.joint + 2u * (1u + c - lay.hub) + 1u).z;
+        }
+        if (c < lay.total) {
+            const unsigned pivot = __float_as_uint(L.get(S.bone + 2u * (c - lay.radius)).x);
+            return L.get(S.node + pivot).z;
+        }
+        return 0.0f;
+    }
+
+    // Copies the constants of the lanes that began a creature (`fresh`)
+    // from their lines into TMEM; the other lanes store back what they
+    // hold. Warp-wide; rare (once a creature).
+    __device__ __forceinline__ static void tm_fill(const Body& b, const TmView& tv, bool fresh) {
+        const unsigned used = min(tv.tm.cols, (tv.lay.total + 3u) & ~3u);
+        for (unsigned c = 0u; c < used; c += 4u) {
+            float4 v = tv.tm.ld4(c);
+            Tmem::wait(v);
+            if (fresh && c < tv.lay.total) {
+                v = make_float4(tm_word(b, tv.lay, c), tm_word(b, tv.lay, c + 1u), tm_word(b, tv.lay, c + 2u),
+                                tm_word(b, tv.lay, c + 3u));
+            }
+            __syncwarp();
+            tv.tm.st4(c, v);
+        }
+        Tmem::wait_st();
+    }
+
+    // Centre of mass x, centre height, lowest and highest point and the
+    // contact and lift bits of the step's end (shaders/creature.cu:1000-1023).
+    struct Tally {
+        bool failed;
+        float center_y, com_x, low, high;
+        unsigned touching, lifted;
+    };
+    __device__ __forceinline__ static void tally_node(const Body& b, Tally& y, unsigned i, const float4& nr) {
+        const float2 q = b.t.pos(i);
+        y.failed = y.failed || !(fabsf(q.x) <= 1e6f && fabsf(q.y) <= 1e6f);
+        y.center_y += q.y;
+        y.com_x += nr.x * q.x;
+        y.low = fminf(y.low, q.y - nr.z);
+        y.high = fmaxf(y.high, q.y + nr.z);
+        if (b.w.has(CE_FLAG_GROUND)) {
+            const float2 g = ground_tally(b.w, q.x, b.r.amp, b.r.qphase, b.p);
+            const float floor_y = __fmaf_rn(nr.z, sqrtf(__fmaf_rn(g.y, g.y, 1.0f)), g.x);
+            if (q.y <= floor_y + kContactSlack) {
+                y.touching |= 1u << i;
+            }
+            if (q.y > floor_y + kLiftClearance) {
+                y.lifted |= 1u << i;
+            }
+        }
+    }
+    __device__ __forceinline__ static Tally tally(const Body& b) {
+        Tally y{false, 0.0f, 0.0f, 1e20f, -1e20f, 0u, 0u};
+        if constexpr (TM) {
+            const unsigned nodes = b.r.nodes;
+            b.template tm_pass<typename Body::NodeRaw>(
+                0u, b.r.wn, [&](unsigned i) { return b.node_fetch(i); }, [&](unsigned i) { return i < nodes; },
+                [&](unsigned i, const typename Body::NodeRaw& n) { tally_node(b, y, i, n.q); });
+        } else {
+            for (unsigned i = 0u; i < b.r.nodes; i++) {
+                tally_node(b, y, i, b.L.get(b.S.node + i));
+            }
+        }
+        return y;
+    }
+
+    // The trial's metrics row and niche cell, from its 19 result words
+    // (niche.cuh: the host's to_metrics and cell index to the bit).
+    __device__ __forceinline__ static void niche_epilogue(const KernelArgs& a, const LaneRegs& r, const float* m) {
+        const ce_result res{m[0],  m[1],  m[2],  m[3],  m[4],  m[5],  m[6],  m[7],  m[8], m[9],
+                            m[10], m[11], m[12], m[13], m[14], m[15], m[16], m[17], m[18]};
+        const ce_metrics mt = to_metrics(res, r.nodes, a.niche);
+        if (a.metrics) {
+            a.metrics[r.cidx] = mt;
+        }
+        a.cells[r.cidx] = cell_of(mt, r.nodes, a.shapes[r.cidx], a.niche);
+    }
+
     // One step of the creature on this lane (shaders/creature.cu:956-1248).
     // Returns whether the lane still has a creature.
-    __device__ __forceinline__ static bool step(const Body& b, const KernelArgs& a) {
+    __device__ __forceinline__ static bool step(const Body& b, const KernelArgs& a, bool live = true) {
         LaneRegs& r = b.r;
         const ce_params& p = b.p;
         const Lines& L = b.L;
@@ -187,28 +301,17 @@ struct Trial {
                 L.put(S.rec_force + i, fl);
             }
         }
-        bool failed = false;
-        float center_y = 0.0f, com_x = 0.0f, low = 1e20f, high = -1e20f;
-        unsigned touching = 0u, lifted = 0u;
-        for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
-            const float2 q = b.t.pos(i);
-            failed = failed || !(fabsf(q.x) <= 1e6f && fabsf(q.y) <= 1e6f);
-            center_y += q.y;
-            com_x += nr.x * q.x;
-            low = fminf(low, q.y - nr.z);
-            high = fmaxf(high, q.y + nr.z);
-            if (b.w.has(CE_FLAG_GROUND)) {
-                const float2 g = ground_tally(b.w, q.x, r.amp, r.qphase, p);
-                const float floor_y = __fmaf_rn(nr.z, sqrtf(__fmaf_rn(g.y, g.y, 1.0f)), g.x);
-                if (q.y <= floor_y + kContactSlack) {
-                    touching |= 1u << i;
-                }
-                if (q.y > floor_y + kLiftClearance) {
-                    lifted |= 1u << i;
-                }
-            }
+        const Tally y = tally(b);
+        // Joints past breaking (warp-wide with TMEM constants, so taken
+        // before the lanes without a creature leave).
+        const bool broken = b.broken_joints() != 0ull;
+        if (!live) {
+            return false;
         }
+        const bool failed = y.failed;
+        float center_y = y.center_y, com_x = y.com_x;
+        const float low = y.low, high = y.high;
+        const unsigned touching = y.touching, lifted = y.lifted;
         center_y /= (float)r.nodes;
         com_x *= r.inv_mass;
         // The result and tallies, from the lane lines.
@@ -281,7 +384,6 @@ struct Trial {
             head_at = h;
             head_vel = v;
         }
-        const bool broken = b.broken_joints() != 0ull;
         bool done = false;
         if (!RECORD || r.scoring) {
             contact_lo = __uint_as_float(contact_bits);
@@ -441,6 +543,9 @@ struct Trial {
                     for (unsigned q = 0u; q < 19u; q++) {
                         __stcs(out + q, m[q]);
                     }
+                    if (!CKPT && a.cells) {
+                        niche_epilogue(a, r, m);
+                    }
                     if (CKPT) {
                         a.ends[r.cidx] = step + 1u;
                     }
@@ -564,11 +669,11 @@ struct Claim {
     }
 };
 
-template <class W, bool RECORD, int RATE, bool CKPT = false>
+template <class W, bool RECORD, int RATE, bool CKPT = false, bool TM = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const KernelArgs a, const ce_params p,
                                                                       const W w) {
     extern __shared__ float4 smem[];
-    using T = Trial<W, RECORD, RATE, CKPT>;
+    using T = Trial<W, RECORD, RATE, CKPT, TM>;
     const unsigned threads = blockDim.x;
     // Tables of rows x threads entries: positions, velocities, forces, then
     // the muscles' (energy, demand) pairs.
@@ -581,21 +686,66 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const Kerne
     const unsigned warps_total = gridDim.x * (threads >> 5u);
     const Lines L{a.scratch + (size_t)warp * S.lines * 32u + lane};
     LaneRegs r;
-    const typename T::Body b{w, p, tab, L, S, r};
     bool live = false;
     Claim claim(a, lane, warp, warps_total);
-    for (;;) {
-        const unsigned mine = claim.next(live);
-        if (mine != kNone) {
-            const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
-            T::begin(b, a, cidx, mine);
-            live = true;
+    if constexpr (TM) {
+        // The block's TMEM: one warp allocates, every warp takes the lanes of
+        // its quarter; freed by the same warp once every warp is done.
+        __shared__ uint32_t tm_base;
+        const unsigned wib = threadIdx.x >> 5u;
+        if (wib == 0u) {
+            tmem_alloc(&tm_base, a.tmem_cols);
         }
-        if (__ballot_sync(kFull, live) == 0u) {
-            break;
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        const Tmem tm{tm_base + (((wib & 3u) * 32u) << 16u), a.tmem_cols};
+        const TmView tv = TmView::make(tm, a.rows, w.has(CE_FLAG_WATER));
+        const typename T::Body b{w, p, tab, L, S, r, &tv};
+        r = LaneRegs{};
+        for (;;) {
+            const unsigned mine = claim.next(live);
+            const bool fresh = mine != kNone;
+            if (fresh) {
+                const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
+                T::begin(b, a, cidx, mine);
+                live = true;
+            }
+            if (__ballot_sync(kFull, live) == 0u) {
+                break;
+            }
+            if (__any_sync(kFull, fresh)) {
+                T::tm_fill(b, tv, fresh);
+            }
+            if (!live) {
+                r.nodes = 0u;
+                r.muscles = 0u;
+            }
+            // (at most the class's node rows, which bound the TMEM layout)
+            r.wn = min(__reduce_max_sync(kFull, r.nodes), a.rows);
+            live = T::step(b, a, live);
         }
-        if (live) {
-            live = T::step(b, a);
+        tmem_fence_before_sync();
+        __syncthreads();
+        if (wib == 0u) {
+            tmem_fence_after_sync();
+            tmem_dealloc(tm_base, a.tmem_cols);
+        }
+    } else {
+        const typename T::Body b{w, p, tab, L, S, r};
+        for (;;) {
+            const unsigned mine = claim.next(live);
+            if (mine != kNone) {
+                const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
+                T::begin(b, a, cidx, mine);
+                live = true;
+            }
+            if (__ballot_sync(kFull, live) == 0u) {
+                break;
+            }
+            if (live) {
+                live = T::step(b, a);
+            }
         }
     }
 }

@@ -402,6 +402,22 @@ ce_status ce_advance_device(ce_engine* engine, const uint32_t* records, const fl
                             uint32_t rate, uint32_t max_nodes, uint32_t max_muscles,
                             void* stream);
 
+/* ce_advance_device with the niche epilogue fused into the creature
+ * kernel: when a creature's trial ends, the kernel stores its result and
+ * also its metrics row (`metrics`, may be NULL) and its dense niche cell
+ * (`cells`, int64, -1 for a shape outside the layout), equal to the host's
+ * ce_to_metrics and ce_niche to the bit, so no pass over the results
+ * follows. `shape_classes` (packed order, from ce_shape_classes) gives each
+ * body's shape class; `world` gives the flags, rate and trial length.
+ * Replaces the host's scheduler::to_metrics and Descriptor::niche_in
+ * (src/scheduler.rs:890-923, src/qd.rs:762-846, 988-999) run after
+ * CudaEngine::poll; the reference kernel itself stores results only. */
+ce_status ce_advance_device_cells(ce_engine* engine, const uint32_t* records, const float* muscles,
+                                  const uint32_t* heads, ce_result* results, uint32_t* counter, void* scratch,
+                                  const ce_params* params, const ce_world* world, uint32_t max_nodes,
+                                  uint32_t max_muscles, const uint8_t* shape_classes, int global_layout,
+                                  ce_metrics* metrics, int64_t* cells, void* stream);
+
 /* Several generations as one CUDA graph (no counterpart in the reference,
  * which launches each wave): the packed batches are copied to the device
  * once; ce_graph_launch runs every generation (node-count bucketing and the

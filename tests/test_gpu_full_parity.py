@@ -17,8 +17,12 @@ reference engine's wave and grid rule):
 
 Equal results give equal niche cells, which the host computes from the
 result fields alone (src/scheduler.rs:890-923, src/qd.rs:795-808); the test
-checks the cells too. It also checks run-to-run repeatability on the GPU
-(tests/gpu_repeatability.rs:18-68 in the reference) on the effects
+checks the cells too. On the game and effects generations it also runs the
+device entry with the niche epilogue fused into the creature kernel
+(ce_advance_device_cells) and checks its results against the reference
+kernel's and its metrics rows and cells against the host's, computed from
+the reference kernel's results. It also checks run-to-run repeatability on
+the GPU (tests/gpu_repeatability.rs:18-68 in the reference) on the effects
 generation, whose claim order varies between runs.
 """
 import numpy as np
@@ -48,6 +52,44 @@ def niche_cells(pop, wave, res, world):
     nodes = (wave.heads[:, 0] & 255).astype(np.uint32)
     metrics = ce.to_metrics(res, nodes, world)
     return ce.niche_cells(pop, metrics, indices=order)
+
+
+def fused_cells(engine, pop, wave, world):
+    """Results, metrics rows and cells of the device entry with the fused
+    niche epilogue (global layout), on device-resident records."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n = len(wave)
+    flags, rate = ce.world_flags(world), world.rate or 60
+    params = ce.make_params(world, 0, n, 0)
+    d_lanes = torch.from_numpy(wave.lanes.view(np.int32)).to(dev)
+    d_muscles = torch.from_numpy(wave.muscles).to(dev)
+    d_heads = torch.from_numpy(wave.heads.view(np.int32).reshape(-1)).to(dev)
+    d_shapes = torch.from_numpy(ce.shape_classes(pop, wave)).to(dev)
+    d_res = torch.full((n * 19,), float("nan"), dtype=torch.float32, device=dev)
+    d_metrics = torch.zeros(n * ce.METRICS_DTYPE.itemsize // 4, dtype=torch.int32, device=dev)
+    d_cells = torch.full((n,), -7, dtype=torch.int64, device=dev)
+    d_counter = torch.zeros(16, dtype=torch.int32, device=dev)
+    d_scratch = torch.empty(engine.scratch_bytes(flags, rate, wave.max_nodes, wave.max_muscles, n),
+                            dtype=torch.uint8, device=dev)
+    engine.advance_device_cells(d_lanes.data_ptr(), d_muscles.data_ptr(), d_heads.data_ptr(), d_res.data_ptr(),
+                                d_counter.data_ptr(), d_scratch.data_ptr(), params, world, wave.max_nodes,
+                                wave.max_muscles, d_shapes.data_ptr(), d_cells.data_ptr(), d_metrics.data_ptr(),
+                                torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize(dev)
+    return (d_res.cpu().numpy().view(ce.RESULT_DTYPE), d_metrics.cpu().numpy().view(ce.METRICS_DTYPE),
+            d_cells.cpu().numpy())
+
+
+def check_fused_cells(engine, pop, wave, world, ref):
+    res, metrics, cells = fused_cells(engine, pop, wave, world)
+    assert_same_bits(res, ref, "fused-epilogue entry against the reference kernel")
+    nodes = (wave.heads[:, 0] & 255).astype(np.uint32)
+    host_m = ce.to_metrics(ref, nodes, world)
+    assert (metrics.view(np.uint32) == host_m.view(np.uint32)).all(), "metrics rows differ from the host's"
+    host_cells = ce.niche_cells(pop, host_m, indices=wave.slots)
+    bad = np.nonzero(cells != host_cells)[0]
+    assert len(bad) == 0, f"{len(bad)} cells differ; first {bad[:5]}: {cells[bad[:5]]} vs {host_cells[bad[:5]]}"
 
 
 def full_generation(engine, name):
@@ -98,6 +140,7 @@ def test_game_workload_full_generation_matches_bits(engine):
     assert len(mine) == 3_000_000
     assert_same_bits(mine, ref, "game workload, 3M x 20 s")
     assert (niche_cells(pop, wave, mine, world) == niche_cells(pop, wave, ref, world)).all()
+    check_fused_cells(engine, pop, wave, world, ref)
     # The trials run long enough to be worth measuring on.
     assert ce.creature_substeps(mine, world) > 0.5 * len(mine) * 1200 * 16
 
@@ -107,5 +150,6 @@ def test_effects_workload_full_generation_matches_bits_and_repeats(engine):
     assert len(mine) == 3_000_000
     assert_same_bits(mine, ref, "effects workload, 3M x 20 s")
     assert (niche_cells(pop, wave, mine, world) == niche_cells(pop, wave, ref, world)).all()
+    check_fused_cells(engine, pop, wave, world, ref)
     again, _ = engine.run(wave, world)
     assert_same_bits(again, mine, "effects workload, second run")
