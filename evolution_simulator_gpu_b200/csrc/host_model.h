@@ -9,14 +9,9 @@ namespace ce {
 extern thread_local std::string g_last_error;
 void set_error(const std::string& msg);
 
-uint32_t quake_hash(uint64_t id);
-float quake_phase(uint32_t h);
-float quake_scale(uint32_t h);
-float terrain_amplitude(uint32_t level);
-uint16_t f32_to_f16(float v);
 float f16_to_f32(uint16_t h);
-void ground(float x, float amplitude, float tilt, float width, float hurdle, float phase, float& h,
-            float& s);
+// The quake hash, terrain amplitude, f32 -> f16 rounding and ground of the
+// packer are in packer.h, shared with the device packer.
 
 bool validate_body(const ce_population& pop, size_t i, std::string* why);
 void fill_creature(const ce_population& pop, size_t i, const ce_world& w, uint32_t* record,
