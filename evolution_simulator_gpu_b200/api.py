@@ -173,6 +173,10 @@ def _bind(lib: C.CDLL) -> None:
         "ce_advance_device_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_void_p, P(Params), P(World), C.c_uint32, C.c_uint32,
                                               C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_pack_plan": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_size_t, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_pack_device": (C.c_int, [P(PopulationC), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                     P(World), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
         "ce_measure_fp32": (C.c_int, [C.c_int, P(C.c_double), P(C.c_double)]),
         "ce_ground": (None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P(C.c_float),
@@ -232,7 +236,7 @@ def lib() -> C.CDLL:
 EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_frame_stride", "ce_generate_size",
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
-            "ce_advance_scratch_bytes", "ce_advance_device", "ce_advance_device_cells", "ce_inject_fault", "ce_measure_fp32",
+            "ce_advance_scratch_bytes", "ce_advance_device", "ce_advance_device_cells", "ce_pack_plan", "ce_pack_device", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
@@ -465,6 +469,43 @@ def pack(pop: Population, world: World, indices=None) -> WavePack:
     _check(L.ce_pack(C.byref(pc), _ptr(idx), n, C.byref(world), _ptr(lanes), _ptr(muscles), _ptr(heads),
                      _ptr(slots), _ptr(info)), "ce_pack")
     return WavePack(lanes, muscles, heads, slots, info)
+
+
+@dataclasses.dataclass
+class PackPlan:
+    """The host half of a device packing (ce_pack_plan): packed order
+    (population indices), record and muscle offsets, 3 floats per bone gene
+    (direction, sine, cosine), and the sizes of the packed arrays."""
+    order: np.ndarray
+    record_at: np.ndarray
+    muscle_at: np.ndarray
+    trig: np.ndarray
+    lanes_len: int
+    muscles_len: int
+
+
+def pack_plan(pop: Population, world: World, indices=None) -> PackPlan:
+    L = lib()
+    pc = pop.c()
+    idx = None if indices is None else np.ascontiguousarray(indices, np.uint32)
+    n = len(pop) if idx is None else len(idx)
+    rl, ml = C.c_size_t(), C.c_size_t()
+    _check(L.ce_pack_size(C.byref(pc), _ptr(idx), n, C.byref(rl), C.byref(ml)), "ce_pack_size")
+    order = np.zeros(n, np.uint32)
+    rat = np.zeros(n, np.uint32)
+    mat = np.zeros(n, np.uint32)
+    trig = np.zeros(3 * max(len(pop.bones), 1), np.float32)
+    _check(L.ce_pack_plan(C.byref(pc), _ptr(idx), n, C.byref(world), len(pop.bones), _ptr(order), _ptr(rat),
+                          _ptr(mat), _ptr(trig)), "ce_pack_plan")
+    return PackPlan(order, rat, mat, trig, rl.value, ml.value)
+
+
+def pack_device(dev_pop: PopulationC, trig: int, order: int, record_at: int, muscle_at: int, n: int, world: World,
+                lanes: int, muscles: int, heads: int, stream: int = 0) -> None:
+    """ce_pack_device on device pointers: `dev_pop` is a PopulationC whose
+    pointers are device addresses (asynchronous on `stream`)."""
+    _check(lib().ce_pack_device(C.byref(dev_pop), trig, order, record_at, muscle_at, n, C.byref(world), lanes,
+                                muscles, heads, stream or None), "ce_pack_device")
 
 
 def frame_stride(max_muscles: int) -> int:

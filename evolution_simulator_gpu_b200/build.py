@@ -32,7 +32,17 @@ NVCC_FLAGS = [
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp"]
 
 CUDA_SOURCES = ["advance.cu", "adjoint.cu", "bucket.cu", "engine.cu", "metrics.cu", "peak.cu", "noalloc.cu",
-                "sample.cu"]
+                "sample.cu", "pack.cu"]
+# The device packer rounds as the host packer: IEEE division and square
+# root, no contraction of multiply-adds.
+IEEE_SOURCES = {"pack.cu"}
+
+
+def file_flags(name: str) -> list[str]:
+    if name not in IEEE_SOURCES:
+        return NVCC_FLAGS
+    swap = {"--prec-div=false": "--prec-div=true", "--prec-sqrt=false": "--prec-sqrt=true", "--fmad=true": "--fmad=false"}
+    return [swap.get(f, f) for f in NVCC_FLAGS]
 CXX_SOURCES = ["host_model.cpp", "generator.cpp"]
 
 
@@ -71,7 +81,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         src, obj = CSRC / name, OBJ / (name + ".o")
         objs.append(obj)
         if force or _stale(obj, src):
-            jobs.append(([nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)],
+            jobs.append(([nvcc(), *ARCH, *file_flags(name), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)],
                          OBJ / (name + ".log")))
     for name in CXX_SOURCES:
         src, obj = CSRC / name, OBJ / (name + ".o")

@@ -317,6 +317,71 @@ extern "C" ce_status ce_pack(const ce_population* pop, const uint32_t* indices, 
     return CE_OK;
 }
 
+// The host half of a device packing: the packed order and record offsets
+// (as ce_pack lays them out) and, per bone gene, the three single-precision
+// library values the device cannot reproduce: the bone's gene-pose
+// direction atan2(dy, dx) and the sine and cosine of its start-pose angle
+// (make_model and start_state call them; recording them here gives the
+// device the same values). They depend on the node genes alone.
+namespace {
+struct RecordAngle {
+    float* out;
+    float operator()(size_t j, float dy, float dx) const {
+        const float a = std::atan2(dy, dx);
+        out[3 * j] = a;
+        return a;
+    }
+};
+struct RecordTrig {
+    float* out;
+    void operator()(size_t j, float th, float& sn, float& cs) const {
+        sn = std::sin(th);
+        cs = std::cos(th);
+        out[3 * j + 1] = sn;
+        out[3 * j + 2] = cs;
+    }
+};
+}  // namespace
+
+extern "C" ce_status ce_pack_plan(const ce_population* pop, const uint32_t* indices, size_t n, const ce_world* w,
+                                  size_t bones_len, uint32_t* order, uint32_t* record_at, uint32_t* muscle_at,
+                                  float* trig) {
+    if (!pop || !w || !order || !record_at || !muscle_at || !trig) {
+        set_error("ce_pack_plan: null argument");
+        return CE_ERR_INVALID;
+    }
+    std::vector<uint32_t> slot;
+    if (!pack_order(pop, indices, n, slot)) return CE_ERR_INVALID;
+    size_t rl = 0, ml = 0;
+    for (size_t c = 0; c < n; c++) {
+        const uint32_t i = indices ? indices[slot[c]] : slot[c];
+        const ce_genome& g = pop->genomes[i];
+        if ((size_t)g.bone_start + g.bone_count > bones_len) {
+            set_error("ce_pack_plan: a genome's bones lie past bones_len");
+            return CE_ERR_INVALID;
+        }
+        order[c] = i;
+        record_at[c] = (uint32_t)rl;
+        muscle_at[c] = (uint32_t)ml;
+        rl += (size_t)g.node_count * CE_NODE_WORDS + (size_t)g.bone_count * CE_BONE_WORDS;
+        ml += (size_t)g.muscle_count * CE_MUSCLE_FIELDS;
+        if (rl > 0xffffffffull || ml > 0xffffffffull) {
+            set_error("ce_pack_plan: batch too large for 32-bit record offsets");
+            return CE_ERR_INVALID;
+        }
+    }
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long c = 0; c < (long long)n; c++) {
+        const ce_genome& gm = pop->genomes[order[c]];
+        float* t = trig + 3 * (size_t)gm.bone_start;
+        const Model M = make_model(pop->nodes + gm.node_start, gm.node_count, pop->bones + gm.bone_start,
+                                   gm.bone_count, pop->muscles + gm.muscle_start, gm.muscle_count, gm.id, *w,
+                                   RecordAngle{t});
+        (void)start_state(M, *w, RecordTrig{t});
+    }
+    return CE_OK;
+}
+
 // ---------------------------------------------------------------- metrics
 // scheduler::trial_steps and to_metrics (src/scheduler.rs:859-923).
 extern "C" ce_status ce_to_metrics(const ce_result* r, uint32_t node_count, const ce_world* w,

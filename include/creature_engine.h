@@ -193,6 +193,31 @@ ce_status ce_pack_size(const ce_population* pop, const uint32_t* indices, size_t
 ce_status ce_pack(const ce_population* pop, const uint32_t* indices, size_t n, const ce_world* world,
                   uint32_t* lanes, float* muscles, uint32_t* heads, uint32_t* slots, uint32_t* info);
 
+/* The host half of packing on the device (the same records as ce_pack,
+ * src/kernel.rs:336-411, 471-593). For the `n` creatures of `indices`
+ * (NULL: every creature) it writes the packed order (`order[c]`: the
+ * population index of packed creature c), each packed creature's record
+ * and muscle offsets (`record_at`, `muscle_at`, n each), and, for every
+ * bone gene of those creatures, three floats at 3 * (bone_start + j): the
+ * bone's gene-pose direction and the sine and cosine of its start-pose
+ * angle, from the C library's single-precision functions as the reference's
+ * Rust host calls them (physics2::Model::new / start, src/physics2.rs:190-399).
+ * `trig` holds 3 * bones_len floats. The plan depends on node and bone genes
+ * only: a batch whose muscle genes or frictions change keeps its plan. */
+ce_status ce_pack_plan(const ce_population* pop, const uint32_t* indices, size_t n, const ce_world* world,
+                       size_t bones_len, uint32_t* order, uint32_t* record_at, uint32_t* muscle_at, float* trig);
+
+/* Packs on the device, one creature a thread, from a plan of ce_pack_plan:
+ * `pop` holds device pointers (genes, optional strength scale), `trig`,
+ * `order`, `record_at`, `muscle_at` are device copies of the plan, and
+ * `lanes`, `muscles`, `heads` (sized as ce_pack_size gives) receive the
+ * records, equal to ce_pack's byte for byte. Asynchronous on `stream`.
+ * Replaces kernel::pack_reusing's fill (src/kernel.rs:529-567), which the
+ * reference runs on host threads. */
+ce_status ce_pack_device(const ce_population* pop, const float* trig, const uint32_t* order,
+                         const uint32_t* record_at, const uint32_t* muscle_at, size_t n, const ce_world* world,
+                         uint32_t* lanes, float* muscles, uint32_t* heads, void* stream);
+
 /* The ground's height and slope under x for bump height `amplitude`, slope
  * `tilt`, pit width `width`, hurdle height `hurdle` and quake phase `phase`
  * (physics::ground, src/physics.rs:668-683), as the packer places creatures
