@@ -165,35 +165,45 @@ struct Trial {
 
     // Word `c` of the TMEM layout of this lane's creature, from the lines
     // that begin() wrote (TmLayout: the same values, laid out for TMEM).
+    // Items past the creature's own (a smaller body than the class's) are
+    // 0: their lines in the slot hold another creature's values, or none.
     __device__ __forceinline__ static float tm_word(const Body& b, const TmLayout& lay, unsigned c) {
         const Lines& L = b.L;
         const SlotLayout& S = b.S;
+        const unsigned nodes = b.r.nodes;
         if (c < lay.bone) {
+            if (c / 4u >= nodes) return 0.0f;
             const float4 v = L.get(S.node + c / 4u);
             const unsigned k = c % 4u;
             return k == 0u ? v.x : k == 1u ? v.y : k == 2u ? v.z : v.w;
         }
         if (c < lay.joint) {
             const unsigned j = (c - lay.bone) / 4u, k = (c - lay.bone) % 4u;
+            if (j + 1u >= nodes) return 0.0f;
             if (k == 3u) return L.get(S.bone + 2u * j + 1u).x;
             const float4 v = L.get(S.bone + 2u * j);
             return k == 0u ? v.x : k == 1u ? v.y : v.z;
         }
         if (c < lay.limit) {
             const unsigned j = 1u + (c - lay.joint) / 4u, k = (c - lay.joint) % 4u;
+            if (j + 1u >= nodes) return 0.0f;
             if (k == 3u) return L.get(S.joint + 2u * j + 1u).y;
             const float4 v = L.get(S.joint + 2u * j);
             return k == 0u ? v.x : k == 1u ? v.y : v.z;
         }
         if (c < lay.hub) {
-            return L.get(S.bone + 2u * (c - lay.limit) + 1u).y;
+            const unsigned j = c - lay.limit;
+            return j + 1u < nodes ? L.get(S.bone + 2u * j + 1u).y : 0.0f;
         }
         if (c < lay.radius) {
-            return L.get(S.joint + 2u * (1u + c - lay.hub) + 1u).z;
+            const unsigned j = 1u + c - lay.hub;
+            return j + 1u < nodes ? L.get(S.joint + 2u * j + 1u).z : 0.0f;
         }
         if (c < lay.total) {
-            const unsigned pivot = __float_as_uint(L.get(S.bone + 2u * (c - lay.radius)).x);
-            return L.get(S.node + pivot).z;
+            const unsigned j = c - lay.radius;
+            if (j + 1u >= nodes) return 0.0f;
+            const unsigned pivot = __float_as_uint(L.get(S.bone + 2u * j).x);
+            return pivot < nodes ? L.get(S.node + pivot).z : 0.0f;
         }
         return 0.0f;
     }
