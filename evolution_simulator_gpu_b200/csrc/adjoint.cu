@@ -1053,14 +1053,14 @@ __global__ void __launch_bounds__(kBlock, 2) adjoint_kernel(const KernelArgs a, 
     float2* const forces = tables + 4u * node_table;
     float* const gmass = reinterpret_cast<float*>(reinterpret_cast<float2*>(smem) + 5u * node_table) + threadIdx.x;
     float2* const muscles = reinterpret_cast<float2*>(smem) + 5u * node_table + node_table / 2u + threadIdx.x;
-    const NodeTables tab{tables, tables + node_table, forces, muscles, threads};
-    const NodeTables adj{tables + 2u * node_table, tables + 3u * node_table, forces, muscles + muscle_table, threads};
+    const NodeTables tab{tables, tables + node_table, forces, muscles};
+    const NodeTables adj{tables + 2u * node_table, tables + 3u * node_table, forces, muscles + muscle_table};
     const SlotLayout S = SlotLayout::make(a.rows, a.mm, false);
     const AdjointLayout A = AdjointLayout::make(a.rows, a.mm);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = (blockIdx.x * threads + threadIdx.x) >> 5u;
     const unsigned warps_total = gridDim.x * (threads >> 5u);
-    const Lines L{a.scratch + (size_t)warp * A.lines * 32u + lane};
+    const Lines L = Lines::make(a.scratch + (size_t)warp * A.lines * 32u, lane);
     const unsigned tl = tape_lines(a.rows, a.mm);
     const Tape tape{x.tape + (size_t)warp * 256u * tl * 32u + lane, tl};
     const W w{};

@@ -20,12 +20,10 @@ static int carveout_for(size_t smem, int blocks) {
     return pct < 1 ? 1 : (pct > 100 ? 100 : pct);
 }
 
-// The kernel of a world, recording switch and step rate: the plain kernel
-// keeps its node, bone and joint constants in TMEM, the recording kernel in
-// the lanes' lines.
+// The kernel of a world, recording switch and step rate.
 template <class W, bool RECORD, int RATE>
 constexpr auto kernel_of() {
-    return advance_kernel<W, RECORD, RATE, false, !RECORD>;
+    return advance_kernel<W, RECORD, RATE>;
 }
 
 template <class W, bool RECORD, int RATE>
@@ -49,12 +47,7 @@ static cudaError_t launch_one(const LaunchSpec& s, const KernelArgs& a, const ce
     e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                              carveout_for(smem, blocks > 0 ? blocks : 1));
     if (e != cudaSuccess) return e;
-    KernelArgs args = a;
-    // TMEM columns of a block: an even share of the 512 among the blocks that
-    // can sit on a multiprocessor at once, so no block waits for columns.
-    const unsigned share = s.sm_share ? s.sm_share : (unsigned)(blocks > 0 ? blocks : 1);
-    args.tmem_cols = tmem_columns(TmLayout::make(s.rows, w.has(CE_FLAG_WATER)).total, share);
-    kern<<<s.grid, s.block, smem, s.stream>>>(args, p, w);
+    kern<<<s.grid, s.block, smem, s.stream>>>(a, p, w);
     return cudaGetLastError();
 }
 

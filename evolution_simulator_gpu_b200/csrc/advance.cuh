@@ -18,49 +18,22 @@
 #pragma once
 #include "kernels.h"
 #include "physics.cuh"
-#include "tmem.cuh"
 
 namespace cek {
 
 constexpr uint32_t kChunk = 32;
 
-// Per-lane values kept in registers across a step. `wn` is the most nodes
-// of any live lane of the warp (the same on every lane), the trip count of
-// the passes whose constants come from TMEM.
+// Per-lane values kept in registers across a step.
 struct LaneRegs {
-    uint32_t nodes, muscles, feet, cidx, step, flags, rec_slot, wn;
+    uint32_t nodes, muscles, feet, cidx, step, flags, rec_slot;
     float amp, qphase, inv_mass, period_f;
     bool limp, scoring;
+    bool tendon;  // a muscle of the creature has a tendon
 };
 
-// A warp's TMEM constants (tmem.cuh): where each kind lives and whether all
-// of that kind fit in the block's columns. A kind that does not fit is read
-// from the lane's lines instead, as without TMEM.
-struct TmView {
-    Tmem tm;
-    TmLayout lay;
-    bool nodes, bones, joints, limits, hubs, radii;
-    __device__ __forceinline__ static TmView make(const Tmem& tm, unsigned ns, bool water) {
-        TmView v;
-        v.tm = tm;
-        v.lay = TmLayout::make(ns, water);
-        v.nodes = v.lay.bone <= tm.cols;
-        v.bones = v.lay.joint <= tm.cols;
-        v.joints = v.lay.limit <= tm.cols;
-        v.limits = v.lay.hub <= tm.cols;
-        v.hubs = v.lay.radius <= tm.cols;
-        v.radii = water && v.lay.total <= tm.cols;
-        return v;
-    }
-};
-
-// ------------------------------------------------------ substep passes
-// TM: the node, bone and joint constants of the substep passes come from
-// TMEM (`tv`), and those passes run warp-uniform trip counts (r.wn) with
-// the lanes whose creature has fewer items idle; otherwise every constant
-// comes from the lane's lines and each lane runs its own trip counts. The
-// arithmetic of an item is the same either way (the *_item functions).
-template <class W, int RATE, bool RECORD, bool TM = false>
+// The arithmetic of each item of a pass sits in its own function (the
+// *_item functions), which the pass loops call.
+template <class W, int RATE, bool RECORD>
 struct Creature {
     using C = Clock<RATE>;
     const W& w;
@@ -69,7 +42,6 @@ struct Creature {
     const Lines& L;
     const SlotLayout& S;
     LaneRegs& r;
-    const TmView* tv = nullptr;
 
     // Joint j from its two lines (shaders/creature.cu:322-356).
     struct Joint {
@@ -157,7 +129,14 @@ struct Creature {
 #pragma unroll 4
         for (unsigned k = 0u; k < r.muscles; k++) {
             const unsigned m0 = S.muscle + 5u * k;
-            const float4 q0 = L.get(m0 + kPull0), q1 = L.get(m0 + kPull1);
+            // The pull lines: (nodes, anchors, hill), then the force cap and
+            // 1/capacity, and the tendon's stiffness and slack only for a
+            // creature that has a tendon (0 and 0 otherwise, which give the
+            // same zero tendon force).
+            const float4 q0 = L.get(m0 + kPull0);
+            const float2 qc = L.get2(S.cap, k);
+            const float2 qt = r.tendon ? L.get2(S.tendon, k) : make_float2(0.0f, 0.0f);
+            const float4 q1 = make_float4(qc.x, qc.y, qt.x, qt.y);
             const float2 ms = t.muscle(k);
             const unsigned nodes = __float_as_uint(q0.x);
             const unsigned a0 = nodes & 255u, a1 = (nodes >> 8u) & 255u, b0 = (nodes >> 16u) & 255u,
@@ -358,173 +337,54 @@ struct Creature {
         t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
     }
 
-    // ------------------------------------------------ TMEM line fetchers
-    // Each fetch issues the loads of one item (TMEM, or the lane's lines for
-    // a kind that does not fit); `wait` makes them usable, after which the
-    // item's lines are assembled in the layout of the lane's lines.
-    struct NodeRaw {
-        float4 q;
-    };
-    __device__ __forceinline__ NodeRaw node_fetch(unsigned i) const {
-        NodeRaw n;
-        n.q = tv->nodes ? tv->tm.ld4(tv->lay.node + 4u * i) : L.get(S.node + i);
-        return n;
-    }
-    __device__ __forceinline__ static void wait(NodeRaw& n) { Tmem::wait(n.q); }
-
-    // Bone j: the quad (pivot, length, 1/m pivot, air factor), 1/m of the
-    // child node, the drag limit and (water) both radii.
-    struct BoneRaw {
-        float4 q;
-        float w1, limit, r0, r1;
-    };
-    template <bool DRAG>
-    __device__ __forceinline__ BoneRaw bone_fetch(unsigned j) const {
-        BoneRaw b;
-        b.limit = b.r0 = b.r1 = 0.0f;
-        if (tv->bones) {
-            b.q = tv->tm.ld4(tv->lay.bone + 4u * j);
-        } else {
-            const float4 ba = L.get(S.bone + 2u * j);
-            b.q = make_float4(ba.x, ba.y, ba.z, DRAG ? L.get(S.bone + 2u * j + 1u).x : 0.0f);
-        }
-        b.w1 = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 1u) : L.get(S.node + j + 1u).y;
-        if (DRAG) {
-            b.limit = tv->limits ? tv->tm.ld1(tv->lay.limit + j) : L.get(S.bone + 2u * j + 1u).y;
-            if (w.has(CE_FLAG_WATER)) {
-                b.r1 = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 2u) : L.get(S.node + j + 1u).z;
-                if (tv->radii) {
-                    b.r0 = tv->tm.ld1(tv->lay.radius + j);
-                }
-            }
-        }
-        return b;
-    }
-    __device__ __forceinline__ static void wait(BoneRaw& b) { Tmem::wait(b.q, b.w1, b.limit, b.r1); }
-    __device__ __forceinline__ float4 bone_a(const BoneRaw& b) const { return make_float4(b.q.x, b.q.y, b.q.z, b.w1); }
-    // The drag scales as the set-up computes them (0.5 h / m).
-    __device__ __forceinline__ float4 bone_b(const BoneRaw& b) const {
-        return make_float4(b.q.w, b.limit, 0.5f * C::h * b.q.z, 0.5f * C::h * b.w1);
-    }
-    __device__ __forceinline__ float bone_r0(const BoneRaw& b) const {
-        if (!w.has(CE_FLAG_WATER)) return 0.0f;
-        return tv->radii ? b.r0 : L.get(S.node + __float_as_uint(b.q.x)).z;
-    }
-
-    // Joint j: the quad (topology, lo, hi, 1/m far node), 1/m of the tip
-    // (node j + 1) and of the hub.
-    struct JointRaw {
-        float4 q;
-        float w_tip, w_hub;
-    };
-    __device__ __forceinline__ JointRaw joint_fetch(unsigned j) const {
-        JointRaw k;
-        if (tv->joints && tv->hubs) {
-            k.q = tv->tm.ld4(tv->lay.joint + 4u * (j - 1u));
-            k.w_hub = tv->tm.ld1(tv->lay.hub + (j - 1u));
-        } else {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
-            k.q = make_float4(ra.x, ra.y, ra.z, rb.y);
-            k.w_hub = rb.z;
-        }
-        k.w_tip = tv->nodes ? tv->tm.ld1(tv->lay.node + 4u * (j + 1u) + 1u) : L.get(S.node + j + 1u).y;
-        return k;
-    }
-    __device__ __forceinline__ static void wait(JointRaw& k) { Tmem::wait(k.q, k.w_tip, k.w_hub); }
-    // The joint's middle angle as the set-up computes it.
-    __device__ __forceinline__ static float4 joint_a(const JointRaw& k) {
-        return make_float4(k.q.x, k.q.y, k.q.z, 0.5f * (k.q.y + k.q.z));
-    }
-    __device__ __forceinline__ static float4 joint_b(const JointRaw& k) {
-        return make_float4(k.w_tip, k.q.w, k.w_hub, 0.0f);
-    }
-
-    // A warp-uniform pass over items first .. last - 1 with the next item's
-    // loads in flight while the current one is worked on. `work(j, raw)`
-    // runs on the lanes whose creature has item j (`has(j)`).
-    template <class Raw, class Fetch, class Has, class Work>
-    __device__ __forceinline__ void tm_pass(unsigned first, unsigned last, Fetch fetch, Has has,
-                                            Work work) const {
-        if (first >= last) {
-            return;
-        }
-        __syncwarp();  // lanes may arrive from loops of their own lengths
-        Raw cur = fetch(first);
-        wait(cur);
-        for (unsigned j = first; j < last; j++) {
-            const unsigned nj = j + 1u < last ? j + 1u : j;
-            Raw nxt = fetch(nj);
-            if (has(j)) {
-                work(j, cur);
-            }
-            __syncwarp();  // the TMEM wait and the next loads are warp-wide
-            wait(nxt);
-            cur = nxt;
-        }
-    }
-
     // ------------------------------------------------------------ passes
     // Air and water drag on the bones (shaders/creature.cu:553-593).
     __device__ __forceinline__ void bone_drag() const {
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<BoneRaw>(
-                0u, r.wn > 0u ? r.wn - 1u : 0u, [&](unsigned j) { return bone_fetch<true>(j); },
-                [&](unsigned j) { return j + 1u < nodes; },
-                [&](unsigned j, const BoneRaw& b) { drag_item(j, bone_a(b), bone_b(b), bone_r0(b), b.r1); });
-        } else {
-            const unsigned bones = r.nodes - 1u;
+        const unsigned bones = r.nodes - 1u;
+        if (w.has(CE_FLAG_WATER)) {
+            // Water drag reads the bone's length and both radii as well.
             float4 na = L.get(S.bone), nb = L.get(S.bone + 1u);
             for (unsigned j = 0u; j < bones; j++) {
                 const float4 ba = na, bb = nb;
                 na = L.get(S.bone + 2u * j + 2u);
                 nb = L.get(S.bone + 2u * j + 3u);
-                float r0 = 0.0f, r1 = 0.0f;
-                if (w.has(CE_FLAG_WATER)) {
-                    r0 = L.get(S.node + __float_as_uint(ba.x)).z;
-                    r1 = L.get(S.node + j + 1u).z;
-                }
+                const float r0 = L.get2(S.ground, __float_as_uint(ba.x)).x, r1 = L.get2(S.ground, j + 1u).x;
                 drag_item(j, ba, bb, r0, r1);
+            }
+        } else {
+            // Air drag needs only the pivot of line a.
+            float na = L.get1(S.pivot, 0u);
+            float4 nb = L.get(S.bone + 1u);
+            for (unsigned j = 0u; j < bones; j++) {
+                const float pivot = na;
+                const float4 bb = nb;
+                na = L.get1(S.pivot, j + 1u);
+                nb = L.get(S.bone + 2u * j + 3u);
+                drag_item(j, make_float4(pivot, 0.0f, 0.0f, 0.0f), bb, 0.0f, 0.0f);
             }
         }
     }
 
     // Bone lengths (shaders/creature.cu:597-613).
     __device__ __forceinline__ void solve_bones() const {
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<BoneRaw>(
-                0u, r.wn > 0u ? r.wn - 1u : 0u, [&](unsigned j) { return bone_fetch<false>(j); },
-                [&](unsigned j) { return j + 1u < nodes; },
-                [&](unsigned j, const BoneRaw& b) { bone_item(j, bone_a(b)); });
-        } else {
-            const unsigned bones = r.nodes - 1u;
-            float4 na = L.get(S.bone);
-            for (unsigned j = 0u; j < bones; j++) {
-                const float4 ba = na;
-                na = L.get(S.bone + 2u * j + 2u);
-                bone_item(j, ba);
-            }
+        const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.bone);
+        for (unsigned j = 0u; j < bones; j++) {
+            const float4 ba = na;
+            na = L.get(S.bone + 2u * j + 2u);
+            bone_item(j, ba);
         }
     }
 
     // Joint ranges (shaders/creature.cu:618-634).
     __device__ __forceinline__ void solve_joints() const {
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<JointRaw>(
-                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
-                [&](unsigned j) { return j + 1u < nodes; },
-                [&](unsigned j, const JointRaw& k) { limit_item(j, joint_a(k), joint_b(k)); });
-        } else {
-            const unsigned bones = r.nodes - 1u;
-            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-            for (unsigned j = 1u; j < bones; j++) {
-                const float4 ra = na, rb = nb;
-                na = L.get(S.joint + 2u * j + 2u);
-                nb = L.get(S.joint + 2u * j + 3u);
-                limit_item(j, ra, rb);
-            }
+        const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
+        for (unsigned j = 1u; j < bones; j++) {
+            const float4 ra = na, rb = nb;
+            na = L.get(S.joint + 2u * j + 2u);
+            nb = L.get(S.joint + 2u * j + 3u);
+            limit_item(j, ra, rb);
         }
     }
 
@@ -572,41 +432,31 @@ struct Creature {
     }
 
     // Joint damping (shaders/creature.cu:683-702).
+    // Damping reads only the topology word of a joint's first line.
     __device__ __forceinline__ void damp_joints() const {
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<JointRaw>(
-                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
-                [&](unsigned j) { return j + 1u < nodes; },
-                [&](unsigned j, const JointRaw& k) { damp_item(j, joint_a(k), joint_b(k)); });
-        } else {
-            const unsigned bones = r.nodes - 1u;
-            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-            for (unsigned j = 1u; j < bones; j++) {
-                const float4 ra = na, rb = nb;
-                na = L.get(S.joint + 2u * j + 2u);
-                nb = L.get(S.joint + 2u * j + 3u);
-                damp_item(j, ra, rb);
-            }
+        const unsigned bones = r.nodes - 1u;
+        float na = L.get1(S.topo, 1u);
+        float4 nb = L.get(S.joint + 3u);
+        for (unsigned j = 1u; j < bones; j++) {
+            const float topo = na;
+            const float4 rb = nb;
+            na = L.get1(S.topo, j + 1u);
+            nb = L.get(S.joint + 2u * j + 3u);
+            damp_item(j, make_float4(topo, 0.0f, 0.0f, 0.0f), rb);
         }
     }
 
     // The per-node passes of a substep: `LAND` false integrates forces,
     // true does ground contact and velocities.
+    // The force pass reads a node's (mass, 1/mass) half line, the ground
+    // pass its (radius, friction) one; a world with water, mud or brambles
+    // (whose forces read the radius) and a recording (whose contact forces
+    // read the mass) read the whole node line.
     template <bool LAND>
     __device__ __forceinline__ void node_pass() const {
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<NodeRaw>(
-                0u, r.wn, [&](unsigned i) { return node_fetch(i); }, [&](unsigned i) { return i < nodes; },
-                [&](unsigned i, const NodeRaw& n) {
-                    if (LAND) {
-                        land_item(i, n.q);
-                    } else {
-                        integrate_item(i, n.q);
-                    }
-                });
-        } else {
+        const bool whole = LAND ? RECORD
+                                : (w.has(CE_FLAG_WATER) || w.has(CE_FLAG_MUD) || w.has(CE_FLAG_BRAMBLES));
+        if (whole) {
             float4 nn = L.get(S.node);
             for (unsigned i = 0u; i < r.nodes; i++) {
                 const float4 nr = nn;
@@ -615,6 +465,18 @@ struct Creature {
                     land_item(i, nr);
                 } else {
                     integrate_item(i, nr);
+                }
+            }
+        } else {
+            const unsigned R = LAND ? S.ground : S.mass;
+            float2 nn = L.get2(R, 0u);
+            for (unsigned i = 0u; i < r.nodes; i++) {
+                const float2 h = nn;
+                nn = L.get2(R, i + 1u);
+                if (LAND) {
+                    land_item(i, make_float4(0.0f, 0.0f, h.x, h.y));
+                } else {
+                    integrate_item(i, make_float4(h.x, h.y, 0.0f, 0.0f));
                 }
             }
         }
@@ -635,26 +497,14 @@ struct Creature {
     // (shaders/creature.cu:746-759).
     __device__ __forceinline__ unsigned long long broken_joints() const {
         unsigned long long bits = 0ull;
-        if constexpr (TM) {
-            const unsigned nodes = r.nodes;
-            tm_pass<JointRaw>(
-                1u, r.wn > 1u ? r.wn - 1u : 1u, [&](unsigned j) { return joint_fetch(j); },
-                [&](unsigned j) { return j + 1u < nodes; },
-                [&](unsigned j, const JointRaw& k) {
-                    if (broken_item(j, joint_a(k), joint_b(k))) {
-                        bits |= 1ull << j;
-                    }
-                });
-        } else {
-            const unsigned bones = r.nodes - 1u;
-            float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
-            for (unsigned j = 1u; j < bones; j++) {
-                const float4 ra = na, rb = nb;
-                na = L.get(S.joint + 2u * j + 2u);
-                nb = L.get(S.joint + 2u * j + 3u);
-                if (broken_item(j, ra, rb)) {
-                    bits |= 1ull << j;
-                }
+        const unsigned bones = r.nodes - 1u;
+        float4 na = L.get(S.joint + 2u), nb = L.get(S.joint + 3u);
+        for (unsigned j = 1u; j < bones; j++) {
+            const float4 ra = na, rb = nb;
+            na = L.get(S.joint + 2u * j + 2u);
+            nb = L.get(S.joint + 2u * j + 3u);
+            if (broken_item(j, ra, rb)) {
+                bits |= 1ull << j;
             }
         }
         return bits;

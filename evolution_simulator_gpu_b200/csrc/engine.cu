@@ -162,12 +162,8 @@ size_t scratch_bytes(unsigned grid, unsigned rows, unsigned mm, bool record) {
 // 2.51 s against 2.77 s one class after the other; at 8 (work 1.12) 4.32 s
 // against 2.96 s; at 10 (0.65) 3.91 s against 2.81 s; at 16 (0.17, 1 small
 // block of 3) 3.87 s against 2.91 s.
-// `shares` receives, per class, how many creature-kernel blocks may share a
-// multiprocessor while it runs (0: its own occupancy), which splits TMEM.
-std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& plans, uint32_t flags, int rate,
-                                  std::vector<unsigned>* shares = nullptr) {
+std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& plans, uint32_t flags, int rate) {
     std::vector<unsigned> grids(plans.size());
-    if (shares) shares->assign(plans.size(), 0u);
     for (size_t c = 0; c < plans.size(); c++) {
         grids[c] = grid_for(e, plans[c].rows, plans[c].mm, flags, false, rate, plans[c].count);
     }
@@ -189,7 +185,6 @@ std::vector<unsigned> class_grids(ce_engine* e, const std::vector<ClassPlan>& pl
     if (2u * small_per_sm < (unsigned)alone_small) return grids;
     grids[0] = std::min<unsigned>(grids[0], small_per_sm * (unsigned)e->sms);
     grids[1] = std::min<unsigned>(grids[1], (unsigned)e->sms);
-    if (shares) shares->assign(2, small_per_sm + 1u);
     return grids;
 }
 
@@ -449,8 +444,7 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
     ce_make_params(w, 0, (uint32_t)pack->count, 0, &p);
     // Grids and scratch of the classes, which run side by side, each with its
     // own part of the slot's scratch.
-    std::vector<unsigned> shares;
-    const std::vector<unsigned> grids = class_grids(e, plans, flags, rate, &shares);
+    const std::vector<unsigned> grids = class_grids(e, plans, flags, rate);
     std::vector<size_t> scratch_at(plans.size());
     size_t scratch = 0;
     for (size_t c = 0; c < plans.size(); c++) {
@@ -496,7 +490,7 @@ extern "C" ce_status ce_submit(ce_engine* e, const ce_wave_pack* pack, const ce_
         a.frames_per_creature = 0;
         a.chunk_k = e->chunk_k;
         cek::LaunchSpec ls{plans[c].rows, plans[c].mm, flags, false, rate, grids[c], cek::kBlock,
-                           c == 0 ? st : sl.side, shares[c]};
+                           c == 0 ? st : sl.side};
         CE_TRY(cek::launch_advance(ls, a, p), "advance launch");
     }
     CE_TRY(cudaEventRecord(sl.joined, sl.side), "cudaEventRecord");
@@ -1061,7 +1055,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
     ce_params p;
     // Plans, grids and scratch of every generation; one scratch a class.
     std::vector<std::vector<ClassPlan>> plans(generations);
-    std::vector<std::vector<unsigned>> grids(generations), shares(generations);
+    std::vector<std::vector<unsigned>> grids(generations);
     size_t scratch_need[2] = {0, 0};
     g->gens.resize(generations);
     for (uint32_t k = 0; k < generations; k++) {
@@ -1071,7 +1065,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
             return fail(CE_ERR_INVALID);
         }
         if ((s = plan_classes(pack, plans[k], e->small_body)) != CE_OK) return fail(s);
-        const std::vector<unsigned> kg = class_grids(e, plans[k], flags, rate, &shares[k]);
+        const std::vector<unsigned> kg = class_grids(e, plans[k], flags, rate);
         for (size_t ci = 0; ci < plans[k].size(); ci++) {
             const ClassPlan& c = plans[k][ci];
             const unsigned grid = kg[ci];
@@ -1132,7 +1126,7 @@ extern "C" ce_status ce_graph_open(ce_engine* e, const ce_wave_pack* packs, uint
             a.mm = plans[k][c].mm;
             a.chunk_k = e->chunk_k;
             cek::LaunchSpec ls{plans[k][c].rows, plans[k][c].mm, flags, false, rate, grids[k][c], cek::kBlock,
-                               c == 0 ? g->stream : g->side, shares[k][c]};
+                               c == 0 ? g->stream : g->side};
             cap = cuda_status(cek::launch_advance(ls, a, p), "advance launch");
         }
         if (cap == CE_OK) cap = cuda_status(cudaEventRecord(g->events[2 * k + 1], g->side), "cudaEventRecord");

@@ -61,7 +61,6 @@ struct KernelArgs {
     float* ckpt;                   // CKPT: checkpoints, ckpt_stride floats a creature (packed index)
     uint32_t ckpt_stride;
     uint32_t* ends;                // CKPT: steps each creature's trial ran (packed index)
-    uint32_t tmem_cols;            // plain kernel: TMEM columns a block allocates (tmem.cuh)
     // Niche epilogue at the result store (plain kernel; `cells` NULL: none):
     // each creature's metrics row (`metrics` may be NULL) and dense cell,
     // from its result, node count and shape class (packed index).
@@ -125,10 +124,6 @@ struct LaunchSpec {
     int rate;        // steps per second: 60 or 120
     unsigned grid, block;
     cudaStream_t stream;
-    // Blocks of creature kernels that may share a multiprocessor while this
-    // launch runs (its own and another launch's beside it), which splits the
-    // 512 TMEM columns; 0: this launch's own occupancy.
-    unsigned sm_share = 0;
 };
 
 // 16-byte lines of one lane's slot.

@@ -238,7 +238,9 @@ struct NodeTables {
     float2* v;   // (vx, vy)
     float2* fp;  // muscle force, then the position at the start of the substep
     float2* ms;  // per muscle: (energy store, demand of the step)
-    unsigned stride;  // threads of the block
+    // Entries between rows: the threads of a block (kBlock), a constant so
+    // that a row's address is one shift and add.
+    static constexpr unsigned stride = 128u;
     __device__ __forceinline__ float4 at(unsigned i) const {
         const float2 q = p[i * stride], u = v[i * stride];
         return make_float4(q.x, q.y, u.x, u.y);
@@ -253,10 +255,25 @@ struct NodeTables {
     __device__ __forceinline__ float2& muscle(unsigned k) const { return ms[k * stride]; }
 };
 
-// The 16-byte constant lines of a lane's creature.
+// The constant lines of a lane's creature: 16-byte lines, and regions of
+// 8-byte half lines and of single words (entry k of a half-line region that
+// starts at line R is float2 R * 64 + k * 32 + lane of the warp's slot, of a
+// word region float R * 128 + k * 32 + lane), so that a warp reads a half
+// line as one 256-byte request and a word as one 128-byte request when a
+// pass needs only part of an item.
 struct Lines {
     float4* base;  // line 0 of this lane
+    float2* half;  // float2 0 of the warp's slot, plus this lane
+    float* words;  // float 0 of the warp's slot, plus this lane
+    __device__ __forceinline__ static Lines make(float4* warp_slot, unsigned lane) {
+        return Lines{warp_slot + lane, reinterpret_cast<float2*>(warp_slot) + lane,
+                     reinterpret_cast<float*>(warp_slot) + lane};
+    }
     __device__ __forceinline__ float4 get(unsigned L) const { return base[L * 32u]; }
+    __device__ __forceinline__ float2 get2(unsigned R, unsigned k) const { return half[R * 64u + k * 32u]; }
+    __device__ __forceinline__ void put2(unsigned R, unsigned k, float2 v) const { half[R * 64u + k * 32u] = v; }
+    __device__ __forceinline__ float get1(unsigned R, unsigned k) const { return words[R * 128u + k * 32u]; }
+    __device__ __forceinline__ void put1(unsigned R, unsigned k, float v) const { words[R * 128u + k * 32u] = v; }
     __device__ __forceinline__ void put(unsigned L, float4 v) const { base[L * 32u] = v; }
     __device__ __forceinline__ float& word(unsigned L, unsigned k) const {
         return reinterpret_cast<float*>(&base[L * 32u])[k];
@@ -280,13 +297,23 @@ struct Lines {
 // contact forces (`rec_force`), the kept result (`rec_kept`, 5 lines) and
 // the muscles' pulls, four to a line (`rec_pull`).
 //
+// The half-line and word regions repeat words of the lines for the passes
+// that need only some of them, so those passes move fewer bytes from L2: a
+// node's (mass, 1/mass) for the force pass (`mass`) and (radius, friction)
+// for the ground pass (`ground`), a muscle's (force cap, 1/capacity)
+// (`cap`) and (tendon stiffness, slack length) (`tendon`, read only for a
+// creature with a tendon), a bone's pivot node for the air drag (`pivot`)
+// and a joint's topology word for the damping (`topo`).
+//
 // The node, bone and joint passes load the line of the next item while they
 // work on the current one, so each loads one item past its last. The
 // regions follow each other (nodes, bones, joints, muscles, then the nine
 // lane lines), so that extra load always lands inside the lane's own slot;
-// a layout that ends with one of those regions needs padding after it.
+// a layout that ends with one of those regions needs padding after it, and
+// each half-line region holds one entry more than it has items.
 struct SlotLayout {
-    unsigned node, bone, joint, muscle, lane, rec_force, rec_kept, rec_pull, lines;
+    unsigned node, bone, joint, muscle, lane, rec_force, rec_kept, rec_pull, mass, ground, cap, tendon, pivot, topo,
+        lines;
     __host__ __device__ static SlotLayout make(unsigned ns, unsigned mm, bool record) {
         SlotLayout s;
         s.node = 0;
@@ -297,7 +324,13 @@ struct SlotLayout {
         s.rec_force = s.lane + 9u;
         s.rec_kept = s.rec_force + ns;
         s.rec_pull = s.rec_kept + 5u;
-        s.lines = record ? s.rec_pull + (mm + 3u) / 4u : s.rec_force;
+        s.mass = record ? s.rec_pull + (mm + 3u) / 4u : s.rec_force;
+        s.ground = s.mass + (ns + 2u) / 2u;
+        s.cap = s.ground + (ns + 2u) / 2u;
+        s.tendon = s.cap + (mm + 2u) / 2u;
+        s.pivot = s.tendon + (mm + 2u) / 2u;
+        s.topo = s.pivot + (ns + 3u) / 4u;
+        s.lines = s.topo + (ns + 3u) / 4u;
         return s;
     }
 };

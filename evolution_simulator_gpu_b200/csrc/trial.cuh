@@ -10,16 +10,12 @@
 namespace cek {
 
 constexpr unsigned kFull = 0xffffffffu;
+static_assert(NodeTables::stride == kBlock, "node table rows are one block wide");
 
-// TM: the creature's node, bone and joint constants come from TMEM (only
-// for the plain kernel, neither recording nor checkpointing); step() is then
-// called by every lane of the warp, `live` telling whether its lane has a
-// creature, since the passes' TMEM loads are warp-wide.
-template <class W, bool RECORD, int RATE, bool CKPT = false, bool TM = false>
+template <class W, bool RECORD, int RATE, bool CKPT = false>
 struct Trial {
-    static_assert(!(TM && (RECORD || CKPT)), "TMEM constants are for the plain kernel");
     using C = Clock<RATE>;
-    using Body = Creature<W, RATE, RECORD, TM>;
+    using Body = Creature<W, RATE, RECORD>;
 
     // Frame t of a recording (shaders/creature.cu:767-779): the reference's
     // frame slots, stored frame-major and creature-minor (slot s of frame t
@@ -90,7 +86,10 @@ struct Trial {
         for (unsigned i = 0u; i < r.nodes; i++) {
             const uint32_t* q = rec + i * CE_NODE_WORDS;
             const float m = __uint_as_float(__ldcs(q + 0));
-            L.put(S.node + i, make_float4(m, 1.0f / m, __uint_as_float(__ldcs(q + 1)), __uint_as_float(__ldcs(q + 2))));
+            const float radius = __uint_as_float(__ldcs(q + 1)), friction = __uint_as_float(__ldcs(q + 2));
+            L.put(S.node + i, make_float4(m, 1.0f / m, radius, friction));
+            L.put2(S.mass, i, make_float2(m, 1.0f / m));
+            L.put2(S.ground, i, make_float2(radius, friction));
             b.t.set_at(i, make_float4(__uint_as_float(__ldcs(q + 3)), __uint_as_float(__ldcs(q + 4)), 0.0f, 0.0f));
             r.feet |= (__ldcs(q + 5) & 1u) << i;
             if (RECORD) {
@@ -124,12 +123,19 @@ struct Trial {
             }
             L.put(S.joint + 2u * j, ra);
             L.put(S.joint + 2u * j + 1u, rb);
+            L.put1(S.pivot, j, __uint_as_float(i0));
+            L.put1(S.topo, j, ra.x);
         }
+        r.tendon = false;
         for (unsigned k = 0u; k < r.muscles; k++) {
             const float4* q = reinterpret_cast<const float4*>(mus + k * CE_MUSCLE_FIELDS);
             const unsigned m0 = S.muscle + 5u * k;
+            const float4 pull1 = __ldcs(q + 1);
             L.put(m0 + kPull0, __ldcs(q + 0));
-            L.put(m0 + kPull1, __ldcs(q + 1));
+            L.put(m0 + kPull1, pull1);
+            L.put2(S.cap, k, make_float2(pull1.x, pull1.y));
+            L.put2(S.tendon, k, make_float2(pull1.z, pull1.w));
+            r.tendon = r.tendon || pull1.z != 0.0f;
             L.put_cold(m0 + kRhythm0, __ldcs(q + 2));
             L.put_cold(m0 + kRhythm1, __ldcs(q + 3));
             L.put_cold(m0 + kMState, make_float4(0.0f, 0.0f, 0.0f, __ldcs(q + 4).x));
@@ -163,69 +169,6 @@ struct Trial {
         }
     }
 
-    // Word `c` of the TMEM layout of this lane's creature, from the lines
-    // that begin() wrote (TmLayout: the same values, laid out for TMEM).
-    // Items past the creature's own (a smaller body than the class's) are
-    // 0: their lines in the slot hold another creature's values, or none.
-    __device__ __forceinline__ static float tm_word(const Body& b, const TmLayout& lay, unsigned c) {
-        const Lines& L = b.L;
-        const SlotLayout& S = b.S;
-        const unsigned nodes = b.r.nodes;
-        if (c < lay.bone) {
-            if (c / 4u >= nodes) return 0.0f;
-            const float4 v = L.get(S.node + c / 4u);
-            const unsigned k = c % 4u;
-            return k == 0u ? v.x : k == 1u ? v.y : k == 2u ? v.z : v.w;
-        }
-        if (c < lay.joint) {
-            const unsigned j = (c - lay.bone) / 4u, k = (c - lay.bone) % 4u;
-            if (j + 1u >= nodes) return 0.0f;
-            if (k == 3u) return L.get(S.bone + 2u * j + 1u).x;
-            const float4 v = L.get(S.bone + 2u * j);
-            return k == 0u ? v.x : k == 1u ? v.y : v.z;
-        }
-        if (c < lay.limit) {
-            const unsigned j = 1u + (c - lay.joint) / 4u, k = (c - lay.joint) % 4u;
-            if (j + 1u >= nodes) return 0.0f;
-            if (k == 3u) return L.get(S.joint + 2u * j + 1u).y;
-            const float4 v = L.get(S.joint + 2u * j);
-            return k == 0u ? v.x : k == 1u ? v.y : v.z;
-        }
-        if (c < lay.hub) {
-            const unsigned j = c - lay.limit;
-            return j + 1u < nodes ? L.get(S.bone + 2u * j + 1u).y : 0.0f;
-        }
-        if (c < lay.radius) {
-            const unsigned j = 1u + c - lay.hub;
-            return j + 1u < nodes ? L.get(S.joint + 2u * j + 1u).z : 0.0f;
-        }
-        if (c < lay.total) {
-            const unsigned j = c - lay.radius;
-            if (j + 1u >= nodes) return 0.0f;
-            const unsigned pivot = __float_as_uint(L.get(S.bone + 2u * j).x);
-            return pivot < nodes ? L.get(S.node + pivot).z : 0.0f;
-        }
-        return 0.0f;
-    }
-
-    // Copies the constants of the lanes that began a creature (`fresh`)
-    // from their lines into TMEM; the other lanes store back what they
-    // hold. Warp-wide; rare (once a creature).
-    __device__ __forceinline__ static void tm_fill(const Body& b, const TmView& tv, bool fresh) {
-        const unsigned used = min(tv.tm.cols, (tv.lay.total + 3u) & ~3u);
-        for (unsigned c = 0u; c < used; c += 4u) {
-            float4 v = tv.tm.ld4(c);
-            Tmem::wait(v);
-            if (fresh && c < tv.lay.total) {
-                v = make_float4(tm_word(b, tv.lay, c), tm_word(b, tv.lay, c + 1u), tm_word(b, tv.lay, c + 2u),
-                                tm_word(b, tv.lay, c + 3u));
-            }
-            __syncwarp();
-            tv.tm.st4(c, v);
-        }
-        Tmem::wait_st();
-    }
-
     // Centre of mass x, centre height, lowest and highest point and the
     // contact and lift bits of the step's end (shaders/creature.cu:1000-1023).
     struct Tally {
@@ -253,15 +196,8 @@ struct Trial {
     }
     __device__ __forceinline__ static Tally tally(const Body& b) {
         Tally y{false, 0.0f, 0.0f, 1e20f, -1e20f, 0u, 0u};
-        if constexpr (TM) {
-            const unsigned nodes = b.r.nodes;
-            b.template tm_pass<typename Body::NodeRaw>(
-                0u, b.r.wn, [&](unsigned i) { return b.node_fetch(i); }, [&](unsigned i) { return i < nodes; },
-                [&](unsigned i, const typename Body::NodeRaw& n) { tally_node(b, y, i, n.q); });
-        } else {
-            for (unsigned i = 0u; i < b.r.nodes; i++) {
-                tally_node(b, y, i, b.L.get(b.S.node + i));
-            }
+        for (unsigned i = 0u; i < b.r.nodes; i++) {
+            tally_node(b, y, i, b.L.get(b.S.node + i));
         }
         return y;
     }
@@ -280,7 +216,7 @@ struct Trial {
 
     // One step of the creature on this lane (shaders/creature.cu:956-1248).
     // Returns whether the lane still has a creature.
-    __device__ __forceinline__ static bool step(const Body& b, const KernelArgs& a, bool live = true) {
+    __device__ __forceinline__ static bool step(const Body& b, const KernelArgs& a) {
         LaneRegs& r = b.r;
         const ce_params& p = b.p;
         const Lines& L = b.L;
@@ -312,12 +248,7 @@ struct Trial {
             }
         }
         const Tally y = tally(b);
-        // Joints past breaking (warp-wide with TMEM constants, so taken
-        // before the lanes without a creature leave).
         const bool broken = b.broken_joints() != 0ull;
-        if (!live) {
-            return false;
-        }
         const bool failed = y.failed;
         float center_y = y.center_y, com_x = y.com_x;
         const float low = y.low, high = y.high;
@@ -679,83 +610,38 @@ struct Claim {
     }
 };
 
-template <class W, bool RECORD, int RATE, bool CKPT = false, bool TM = false>
+template <class W, bool RECORD, int RATE, bool CKPT = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) advance_kernel(const KernelArgs a, const ce_params p,
                                                                       const W w) {
     extern __shared__ float4 smem[];
-    using T = Trial<W, RECORD, RATE, CKPT, TM>;
+    using T = Trial<W, RECORD, RATE, CKPT>;
     const unsigned threads = blockDim.x;
     // Tables of rows x threads entries: positions, velocities, forces, then
     // the muscles' (energy, demand) pairs.
     float2* const tables = reinterpret_cast<float2*>(smem) + threadIdx.x;
     const size_t table = (size_t)a.rows * threads;
-    const NodeTables tab{tables, tables + table, tables + 2u * table, tables + 3u * table, threads};
+    const NodeTables tab{tables, tables + table, tables + 2u * table, tables + 3u * table};
     const SlotLayout S = SlotLayout::make(a.rows, a.mm, RECORD);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = (blockIdx.x * threads + threadIdx.x) >> 5u;
     const unsigned warps_total = gridDim.x * (threads >> 5u);
-    const Lines L{a.scratch + (size_t)warp * S.lines * 32u + lane};
+    const Lines L = Lines::make(a.scratch + (size_t)warp * S.lines * 32u, lane);
     LaneRegs r;
+    const typename T::Body b{w, p, tab, L, S, r};
     bool live = false;
     Claim claim(a, lane, warp, warps_total);
-    if constexpr (TM) {
-        // The block's TMEM: one warp allocates, every warp takes the lanes of
-        // its quarter; freed by the same warp once every warp is done.
-        __shared__ uint32_t tm_base;
-        const unsigned wib = threadIdx.x >> 5u;
-        if (wib == 0u) {
-            tmem_alloc(&tm_base, a.tmem_cols);
+    for (;;) {
+        const unsigned mine = claim.next(live);
+        if (mine != kNone) {
+            const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
+            T::begin(b, a, cidx, mine);
+            live = true;
         }
-        tmem_fence_before_sync();
-        __syncthreads();
-        tmem_fence_after_sync();
-        const Tmem tm{tm_base + (((wib & 3u) * 32u) << 16u), a.tmem_cols};
-        const TmView tv = TmView::make(tm, a.rows, w.has(CE_FLAG_WATER));
-        const typename T::Body b{w, p, tab, L, S, r, &tv};
-        r = LaneRegs{};
-        for (;;) {
-            const unsigned mine = claim.next(live);
-            const bool fresh = mine != kNone;
-            if (fresh) {
-                const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
-                T::begin(b, a, cidx, mine);
-                live = true;
-            }
-            if (__ballot_sync(kFull, live) == 0u) {
-                break;
-            }
-            if (__any_sync(kFull, fresh)) {
-                T::tm_fill(b, tv, fresh);
-            }
-            if (!live) {
-                r.nodes = 0u;
-                r.muscles = 0u;
-            }
-            // (at most the class's node rows, which bound the TMEM layout)
-            r.wn = min(__reduce_max_sync(kFull, r.nodes), a.rows);
-            live = T::step(b, a, live);
+        if (__ballot_sync(kFull, live) == 0u) {
+            break;
         }
-        tmem_fence_before_sync();
-        __syncthreads();
-        if (wib == 0u) {
-            tmem_fence_after_sync();
-            tmem_dealloc(tm_base, a.tmem_cols);
-        }
-    } else {
-        const typename T::Body b{w, p, tab, L, S, r};
-        for (;;) {
-            const unsigned mine = claim.next(live);
-            if (mine != kNone) {
-                const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
-                T::begin(b, a, cidx, mine);
-                live = true;
-            }
-            if (__ballot_sync(kFull, live) == 0u) {
-                break;
-            }
-            if (live) {
-                live = T::step(b, a);
-            }
+        if (live) {
+            live = T::step(b, a);
         }
     }
 }
