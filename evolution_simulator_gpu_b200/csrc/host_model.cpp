@@ -596,111 +596,8 @@ extern "C" ce_status ce_gene_gradients(const ce_population* pop, const uint32_t*
             set_error("ce_gene_gradients: creature larger than the gradient rows");
             return CE_ERR_INVALID;
         }
-        const ce_node_gene* ng = pop->nodes + gm.node_start;
-        const ce_bone_gene* bg = pop->bones + gm.bone_start;
-        const ce_muscle_gene* mg = pop->muscles + gm.muscle_start;
-        const Model M = make_model(ng, gm.node_count, bg, gm.bone_count, mg, gm.muscle_count, gm.id, *world);
-        const float* rec = grads + c * per;
-        const size_t n = gm.node_count, nb = gm.bone_count, nm = gm.muscle_count;
-        // d J / d (gene node mass): the kernel's rows, then the strengths.
-        const Inline<PNode, kNodesMax> body = body_nodes(ng, n, bg, nb, mg, nm);
-        std::vector<uint32_t> row_of(n, 0);
-        row_of[0] = 0;
-        for (size_t j = 0; j < nb; j++) row_of[bg[j].b] = (uint32_t)(j + 1);
-        std::vector<double> dmass(n, 0.0);
-        for (size_t node = 0; node < n; node++) dmass[node] = rec[9 * mm + rows + row_of[node]];
-        // The start pose is moved by minus the centre of mass's x
-        // (start_state), so a mass moves every start x by -x_start / total;
-        // on uneven ground it is also lowered onto the ground under its
-        // lowest node, whose height moves with the shift by the ground's
-        // slope there.
-        {
-            const State st = start_state(M, *world);
-            double shift = 0.0, lift = 0.0;
-            for (size_t r = 0; r < n; r++) {
-                shift += rec[9 * mm + 2 * rows + 2 * r];
-                lift += rec[9 * mm + 2 * rows + 2 * r + 1];
-            }
-            if (world->ground) {
-                float lowest = std::numeric_limits<float>::infinity(), slope = 0.0f;
-                for (size_t r = 0; r < n; r++) {
-                    float h, sl;
-                    ground(st.px[r], M.amplitude, world->slope, world->gaps, world->hurdles, M.quake_phase_, h, sl);
-                    const float low = st.py[r] - M.radius[r] - fmax_(h, -1e6f);
-                    if (low < lowest) {
-                        lowest = low;
-                        slope = sl;
-                    }
-                }
-                shift += lift * (double)slope;
-            }
-            for (size_t node = 0; node < n; node++) {
-                dmass[node] -= shift * (double)st.px[row_of[node]] * (double)M.inv_mass;
-            }
-        }
-        std::vector<double> subtree(nb, 0.0);
-        for (size_t j = 0; j < nb; j++) subtree[j] = body[bg[j].b].mass + (j == 0 ? body[0].mass : 0.0f);
-        for (size_t j = nb; j-- > 1;) {
-            if (M.parent[j] >= 0) subtree[(size_t)M.parent[j]] += subtree[j];
-        }
-        auto within = [&](size_t bone, size_t top) {  // bone in the subtree of bone `top`
-            for (int64_t at = (int64_t)bone; at >= 0; at = M.parent[(size_t)at]) {
-                if ((size_t)at == top) return true;
-                if (at == 0) break;
-            }
-            return false;
-        };
-        for (size_t q = 0; q < nm; q++) {
-            const double driven = std::min(subtree[mg[q].bone_a], subtree[mg[q].bone_b]);
-            const size_t top = subtree[mg[q].bone_a] <= subtree[mg[q].bone_b] ? mg[q].bone_a : mg[q].bone_b;
-            if (!(kDrivenAcceleration * driven / lim::muscle_force < 1.0) || driven <= 0.0) continue;
-            const double strength = M.muscles[q].strength;
-            const double scale = pop->strength_scale ? pop->strength_scale[gm.muscle_start + q] : 1.0;
-            const double d_strength = (double)rec[9 * q + 2] * lim::muscle_force * scale -
-                                      (double)rec[9 * q + 3] / (lim::muscle_energy * strength * strength * scale);
-            const double per_mass = d_strength * strength / driven;
-            if (top == 0) dmass[0] += per_mass;
-            for (size_t i = 0; i < nb; i++) {
-                if (within(i, top)) dmass[bg[i].b] += per_mass;
-            }
-        }
-        for (size_t k = 0; k < gm.muscle_count; k++) {
-            const ce_muscle_gene& m = mg[k];
-            const double g_amp = rec[9 * k + 0], g_hill = rec[9 * k + 1], g_cap = rec[9 * k + 2];
-            const double g_icap = rec[9 * k + 3], g_phase = rec[9 * k + 4], g_duty = rec[9 * k + 5];
-            const double g_iduty = rec[9 * k + 6], g_icomp = rec[9 * k + 7];
-            const float stroke = 2.0f * lim::muscle_speed * m.period * fmin_(m.duty, 1.0f - m.duty) / kPi;
-            const bool by_lengths = (m.long_len - m.short_len) <= stroke;
-            const double T = m.period, duty = m.duty;
-            double d_duty = g_duty - g_iduty / (duty * duty) + g_icomp / ((1.0 - duty) * (1.0 - duty));
-            if (!by_lengths) {
-                d_duty += g_amp * 2.0 * lim::muscle_speed * T / kPi * (m.duty < 1.0f - m.duty ? 1.0 : -1.0);
-            }
-            const bool free_duty = m.duty > 0.05f && m.duty < 0.95f;
-            const double strength = M.muscles[k].strength;
-            const double scale = pop->strength_scale ? pop->strength_scale[gm.muscle_start + k] : 1.0;
-            double* out = muscle_grads + 5 * (gm.muscle_start + k);
-            out[0] = by_lengths ? -g_amp : 0.0;
-            out[1] = (by_lengths ? g_amp : 0.0) +
-                     (m.long_len > 0.05f ? -g_hill / (kHillSpeed * (double)m.long_len * m.long_len) : 0.0);
-            if (m.long_len >= muscle_span(bg, nb, body.data(), n, m)) {
-                const uint32_t bb[2] = {m.bone_a, m.bone_b};
-                const float tt[2] = {m.anchor_a, m.anchor_b};
-                for (int side = 0; side < 2; side++) {
-                    if (bb[side] >= nb || bg[bb[side]].a >= n || bg[bb[side]].b >= n) continue;
-                    const double t = clampf(tt[side], 0.0f, 1.0f);
-                    out[1] += 0.5 * kMuscleMassPerM * ((1.0 - t) * dmass[bg[bb[side]].a] + t * dmass[bg[bb[side]].b]);
-                }
-            }
-            out[2] = g_cap * lim::muscle_force * strength -
-                     g_icap / (lim::muscle_energy * strength * scale * scale);
-            out[3] = -g_phase / T - (free_duty ? d_duty / T : 0.0);
-            out[4] = free_duty ? d_duty / T : 0.0;
-        }
-        for (size_t r = 0; r < gm.node_count; r++) {
-            const size_t gene_node = r == 0 ? 0 : bg[r - 1].b;
-            node_grads[gm.node_start + gene_node] = rec[9 * mm + r];
-        }
+        gene_gradients_one(*pop, (uint32_t)i, *world, grads + c * per, rows, mm, muscle_grads, node_grads,
+                           HostAngle{}, HostTrig{});
     }
     return CE_OK;
 }
