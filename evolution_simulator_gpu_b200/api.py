@@ -177,6 +177,12 @@ def _bind(lib: C.CDLL) -> None:
                                    C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_pack_device": (C.c_int, [P(PopulationC), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                      P(World), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_ascent_open": (C.c_int, [C.c_void_p, P(PopulationC), P(World), C.c_uint32, C.c_double, C.c_size_t,
+                                     C.c_size_t, C.c_size_t, P(C.c_void_p)]),
+        "ce_ascent_launch": (C.c_int, [C.c_void_p, P(C.c_double)]),
+        "ce_ascent_fitness": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),
+        "ce_ascent_genes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_ascent_close": (C.c_int, [C.c_void_p]),
         "ce_inject_fault": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int]),
         "ce_measure_fp32": (C.c_int, [C.c_int, P(C.c_double), P(C.c_double)]),
         "ce_ground": (None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, P(C.c_float),
@@ -236,7 +242,8 @@ def lib() -> C.CDLL:
 EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_frame_stride", "ce_generate_size",
             "ce_generate", "ce_to_metrics", "ce_niche", "ce_open", "ce_close", "ce_last_error", "ce_submit",
             "ce_poll", "ce_wait", "ce_free_slots", "ce_allocated_bytes", "ce_release_idle", "ce_record",
-            "ce_advance_scratch_bytes", "ce_advance_device", "ce_advance_device_cells", "ce_pack_plan", "ce_pack_device", "ce_inject_fault", "ce_measure_fp32",
+            "ce_advance_scratch_bytes", "ce_advance_device", "ce_advance_device_cells", "ce_pack_plan", "ce_pack_device", "ce_ascent_open", "ce_ascent_launch",
+            "ce_ascent_fitness", "ce_ascent_genes", "ce_ascent_close", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
@@ -658,6 +665,58 @@ class Engine:
                                              C.byref(params), C.byref(world), max_nodes, max_muscles, shapes,
                                              1 if global_layout else 0, metrics or None, cells, stream or None),
                "ce_advance_device_cells")
+
+
+# ------------------------------------------------------------------ ascent
+class Ascent:
+    """A population's gradient ascent kept on the GPU (ce_ascent_open):
+    `launch()` runs `steps` checkpointed forward + backward runs, gene
+    gradients, clipped ascent steps and device repacking, then scores the
+    last genes, as one CUDA graph, and returns its GPU seconds;
+    `fitness(k)` is step k's fitness in population order (k = steps: the
+    last genes); `population()` the genes after the steps."""
+
+    def __init__(self, engine: "Engine", pop: Population, world: World, steps: int, step: float):
+        self._pop = pop
+        self.steps = steps
+        h = C.c_void_p()
+        _check(lib().ce_ascent_open(engine.handle, C.byref(pop.c()), C.byref(world), steps, step, len(pop.nodes),
+                                    len(pop.bones), len(pop.muscles), C.byref(h)), "ce_ascent_open")
+        self._h = h
+
+    def launch(self) -> float:
+        s = C.c_double()
+        _check(lib().ce_ascent_launch(self._h, C.byref(s)), "ce_ascent_launch")
+        return s.value
+
+    def fitness(self, step: int) -> np.ndarray:
+        out = np.zeros(len(self._pop), np.float32)
+        _check(lib().ce_ascent_fitness(self._h, step, _ptr(out), len(out)), "ce_ascent_fitness")
+        return out
+
+    def population(self) -> Population:
+        p = self._pop
+        nodes, muscles = p.nodes.copy(), p.muscles.copy()
+        strength = None if p.strength is None else p.strength.copy()
+        _check(lib().ce_ascent_genes(self._h, _ptr(nodes), _ptr(muscles), _ptr(strength)), "ce_ascent_genes")
+        return Population(nodes, p.bones.copy(), muscles, p.genomes.copy(), strength)
+
+    def close(self) -> None:
+        if self._h:
+            lib().ce_ascent_close(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self) -> "Ascent":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------------ graphs

@@ -33,8 +33,9 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 
 CUDA_SOURCES = ["advance.cu", "adjoint.cu", "bucket.cu", "engine.cu", "metrics.cu", "peak.cu", "noalloc.cu",
                 "sample.cu", "pack.cu"]
-# The device packer rounds as the host packer: IEEE division and square
-# root, no contraction of multiply-adds.
+# The device packer, gene gradients and ascent step round as their host
+# counterparts: IEEE division and square root, no contraction of
+# multiply-adds.
 IEEE_SOURCES = {"pack.cu"}
 
 

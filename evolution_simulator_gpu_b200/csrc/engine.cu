@@ -989,6 +989,280 @@ extern "C" ce_status ce_tape_checkpoints(ce_tape* t, float* out, size_t cap_floa
     return CE_OK;
 }
 
+// ------------------------------------------------------ refinement ascent
+// A batch's gradient ascent kept on the device and run as one CUDA graph:
+// per step the checkpointed forward run (which scores the step's genes),
+// the backward run, the gene gradients, the clipped ascent step on the
+// genes and the repacking of the records from them; then a plain run scores
+// the last genes. The host packs once (its plan: order, offsets and the C
+// library's trig values, which the steps never change) and reads the
+// fitness of every step and the final genes at the end.
+struct ce_ascent {
+    ce_engine* engine = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    size_t count = 0, nodes_len = 0, bones_len = 0, muscles_len = 0;
+    unsigned rows = 2, mm = 0, ckpts = 0, steps = 0;
+    uint32_t flags = 0;
+    int rate = 60;
+    ce_params params{};
+    ce_world world{};
+    bool has_strength = false;
+    std::vector<uint32_t> order;
+    DeviceBuf d_nodes, d_bones, d_muscle_genes, d_genomes, d_strength, d_trig, d_order, d_rat, d_mat;
+    DeviceBuf d_lanes, d_muscles, d_heads, d_buckets, d_ckpt, d_ends, d_scratch, d_tape, d_grads, d_mg, d_ng;
+    std::vector<DeviceBuf> d_results;  // one a step, then the last genes' run
+};
+
+extern "C" ce_status ce_ascent_close(ce_ascent* a) {
+    if (!a) return CE_OK;
+    if (a->engine) cudaSetDevice(a->engine->device);
+    if (a->stream) cudaStreamSynchronize(a->stream);
+    if (a->exec) cudaGraphExecDestroy(a->exec);
+    if (a->graph) cudaGraphDestroy(a->graph);
+    for (DeviceBuf* b : {&a->d_nodes, &a->d_bones, &a->d_muscle_genes, &a->d_genomes, &a->d_strength, &a->d_trig,
+                         &a->d_order, &a->d_rat, &a->d_mat, &a->d_lanes, &a->d_muscles, &a->d_heads, &a->d_buckets,
+                         &a->d_ckpt, &a->d_ends, &a->d_scratch, &a->d_tape, &a->d_grads, &a->d_mg, &a->d_ng}) {
+        b->release();
+    }
+    for (DeviceBuf& b : a->d_results) b.release();
+    if (a->start) cudaEventDestroy(a->start);
+    if (a->stop) cudaEventDestroy(a->stop);
+    if (a->stream) cudaStreamDestroy(a->stream);
+    delete a;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_ascent_open(ce_engine* e, const ce_population* pop, const ce_world* w, uint32_t steps,
+                                    double step_size, size_t nodes_len, size_t bones_len, size_t muscles_len,
+                                    ce_ascent** out) {
+    if (!e || !pop || !out || !pop->count || steps == 0) {
+        set_error("ce_ascent_open: null argument, empty population or no step");
+        return CE_ERR_INVALID;
+    }
+    *out = nullptr;
+    ce_status s = check_world(w);
+    if (s != CE_OK) return s;
+    const uint32_t flags = ce_world_flags(w);
+    if (!cek::gradient_world(flags)) {
+        set_error("ce_ascent_open: gradients are built for the calm world and the effects worlds (without mud, "
+                  "brambles or gaps)");
+        return CE_ERR_UNSUPPORTED;
+    }
+    for (size_t k = 0; k < muscles_len; k++) {
+        if (pop->muscles[k].sensor != CE_NO_SENSOR) {
+            set_error("ce_ascent_open: muscles with touch sensors are not differentiated");
+            return CE_ERR_UNSUPPORTED;
+        }
+    }
+    ce_ascent* a = new ce_ascent;
+    auto fail = [&](ce_status st) {
+        ce_ascent_close(a);
+        return st;
+    };
+    a->engine = e;
+    a->count = pop->count;
+    a->nodes_len = nodes_len;
+    a->bones_len = bones_len;
+    a->muscles_len = muscles_len;
+    a->steps = steps;
+    a->flags = flags;
+    a->world = *w;
+    a->rate = (int)ce::world_rate(*w);
+    a->has_strength = pop->strength_scale != nullptr;
+    // The host plan, and a host packing for the sizes and body checks.
+    const size_t n = pop->count;
+    size_t lanes_len = 0, mus_len = 0;
+    if ((s = ce_pack_size(pop, nullptr, n, &lanes_len, &mus_len)) != CE_OK) return fail(s);
+    std::vector<uint32_t> lanes(lanes_len), heads(8 * n), rat(n), mat(n);
+    std::vector<float> muscles(mus_len), trig(3 * std::max<size_t>(bones_len, 1));
+    a->order.resize(n);
+    if ((s = ce_pack_plan(pop, nullptr, n, w, bones_len, a->order.data(), rat.data(), mat.data(), trig.data())) !=
+            CE_OK ||
+        (s = ce_pack(pop, nullptr, n, w, lanes.data(), muscles.data(), heads.data(), nullptr, nullptr)) != CE_OK) {
+        return fail(s);
+    }
+    ce_wave_pack wp{lanes.data(), lanes_len, muscles.data(), mus_len, heads.data(), n};
+    std::vector<ClassPlan> plans;
+    if ((s = plan_classes(&wp, plans)) != CE_OK) return fail(s);
+    for (const ClassPlan& c : plans) {
+        a->rows = std::max(a->rows, c.rows);
+        a->mm = std::max(a->mm, c.mm);
+    }
+    if (cek::adjoint_smem_bytes(a->rows, a->mm, cek::kBlock) > e->smem_optin) {
+        set_error("ce_ascent_open: bodies too large for the backward pass's shared memory");
+        return fail(CE_ERR_UNSUPPORTED);
+    }
+    ce_make_params(w, 0, (uint32_t)n, 0, &a->params);
+    a->ckpts = (a->params.steps + 15u) / 16u;
+    if ((s = set_device(e)) != CE_OK) return fail(s);
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (s = cuda_status(cudaEventCreate(&a->start), "cudaEventCreate")) ||
+        (s = cuda_status(cudaEventCreate(&a->stop), "cudaEventCreate"))) {
+        return fail(s);
+    }
+    // Launch shapes: the forward grid as ce_forward's, the backward as ce_backward's.
+    const unsigned fgrid = grid_for(e, a->rows, a->mm, flags, false, a->rate, n);
+    int per_sm = 0;
+    if (cek::adjoint_occupancy(a->rows, a->mm, flags, a->rate, &per_sm) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const unsigned bgrid =
+        (unsigned)std::max<size_t>(1, std::min((n + cek::kBlock - 1) / cek::kBlock, (size_t)per_sm * e->sms));
+    const size_t per_grad = cek::grad_floats(a->rows, a->mm);
+    const size_t res_b = n * sizeof(ce_result);
+    auto up = [&](DeviceBuf& d, const void* src, size_t bytes) -> ce_status {
+        ce_status st = d.ensure(std::max<size_t>(bytes, 4));
+        if (st != CE_OK) return st;
+        return bytes ? cuda_status(cudaMemcpy(d.ptr, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy") : CE_OK;
+    };
+    if ((s = up(a->d_nodes, pop->nodes, nodes_len * sizeof(ce_node_gene))) ||
+        (s = up(a->d_bones, pop->bones, bones_len * sizeof(ce_bone_gene))) ||
+        (s = up(a->d_muscle_genes, pop->muscles, muscles_len * sizeof(ce_muscle_gene))) ||
+        (s = up(a->d_genomes, pop->genomes, n * sizeof(ce_genome))) ||
+        (s = up(a->d_strength, pop->strength_scale, a->has_strength ? muscles_len * 4 : 0)) ||
+        (s = up(a->d_trig, trig.data(), trig.size() * 4)) || (s = up(a->d_order, a->order.data(), n * 4)) ||
+        (s = up(a->d_rat, rat.data(), n * 4)) || (s = up(a->d_mat, mat.data(), n * 4)) ||
+        (s = up(a->d_lanes, lanes.data(), lanes_len * 4)) || (s = up(a->d_muscles, muscles.data(), mus_len * 4)) ||
+        (s = up(a->d_heads, heads.data(), n * 32)) || (s = a->d_buckets.ensure(cek::bucket_bytes(n))) ||
+        (s = a->d_ckpt.ensure(n * (size_t)a->ckpts * cek::checkpoint_floats(a->rows, a->mm) * 4)) ||
+        (s = a->d_ends.ensure(n * 4)) ||
+        (s = a->d_scratch.ensure(std::max(scratch_bytes(fgrid, a->rows, a->mm, false),
+                                          cek::adjoint_slot_bytes(bgrid, a->rows, a->mm)))) ||
+        (s = a->d_tape.ensure(cek::adjoint_tape_bytes(bgrid, a->rows, a->mm))) ||
+        (s = a->d_grads.ensure(n * per_grad * 4)) || (s = a->d_mg.ensure(std::max<size_t>(muscles_len, 1) * 5 * 8)) ||
+        (s = a->d_ng.ensure(std::max<size_t>(nodes_len, 1) * 8))) {
+        return fail(s);
+    }
+    a->d_results.resize(steps + 1u);
+    for (DeviceBuf& b : a->d_results) {
+        if ((s = b.ensure(res_b)) != CE_OK) return fail(s);
+    }
+    ce_population dpop{static_cast<const ce_node_gene*>(a->d_nodes.ptr), static_cast<const ce_bone_gene*>(a->d_bones.ptr),
+                       static_cast<const ce_muscle_gene*>(a->d_muscle_genes.ptr),
+                       static_cast<const ce_genome*>(a->d_genomes.ptr), n,
+                       a->has_strength ? static_cast<const float*>(a->d_strength.ptr) : nullptr};
+    const cek::Buckets bk = cek::bucket_layout(a->d_buckets.ptr, n);
+    auto args = [&](size_t result) {
+        cek::KernelArgs k{};
+        k.records = static_cast<const uint32_t*>(a->d_lanes.ptr);
+        k.muscles = static_cast<const float*>(a->d_muscles.ptr);
+        k.heads = static_cast<const uint4*>(a->d_heads.ptr);
+        k.results = static_cast<ce_result*>(a->d_results[result].ptr);
+        k.counter = bk.counters;
+        k.scratch = static_cast<float4*>(a->d_scratch.ptr);
+        k.order = bk.order;
+        k.bounds = bk.bounds;
+        k.work = bk.work;
+        k.queues = cek::kQueues;
+        k.count = (uint32_t)n;
+        k.rows = a->rows;
+        k.mm = a->mm;
+        k.chunk_k = e->chunk_k;
+        k.ckpt = static_cast<float*>(a->d_ckpt.ptr);
+        k.ckpt_stride = a->ckpts * cek::checkpoint_floats(a->rows, a->mm);
+        k.ends = static_cast<uint32_t*>(a->d_ends.ptr);
+        return k;
+    };
+    const cudaStream_t st = a->stream;
+    if ((s = cuda_status(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture")))
+        return fail(s);
+    cudaError_t ce = cudaSuccess;
+    const auto* heads_d = static_cast<const uint4*>(a->d_heads.ptr);
+    for (uint32_t k = 0; k < steps && ce == cudaSuccess; k++) {
+        const cek::KernelArgs ka = args(k);
+        const cek::LaunchSpec fs{a->rows, a->mm, flags, false, a->rate, fgrid, cek::kBlock, st};
+        const cek::LaunchSpec bs{a->rows, a->mm, flags, false, a->rate, bgrid, cek::kBlock, st};
+        if (ce == cudaSuccess) ce = cek::launch_bucket(heads_d, 0u, (uint32_t)n, bk, st);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(a->d_ends.ptr, 0, n * 4, st);
+        if (ce == cudaSuccess) ce = cek::launch_forward_ckpt(fs, ka, a->params);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(a->d_grads.ptr, 0, n * per_grad * 4, st);
+        if (ce == cudaSuccess) ce = cek::launch_bucket(heads_d, 0u, (uint32_t)n, bk, st);
+        if (ce == cudaSuccess)
+            ce = cek::launch_adjoint(bs, ka, a->params, static_cast<float4*>(a->d_tape.ptr),
+                                     static_cast<float*>(a->d_grads.ptr), nullptr);
+        if (ce == cudaSuccess)
+            ce = cek::launch_gene_grads(dpop, static_cast<const float*>(a->d_trig.ptr),
+                                        static_cast<const uint32_t*>(a->d_order.ptr), n, a->world,
+                                        static_cast<const float*>(a->d_grads.ptr), a->rows, a->mm,
+                                        static_cast<double*>(a->d_mg.ptr), static_cast<double*>(a->d_ng.ptr), st);
+        if (ce == cudaSuccess)
+            ce = cek::launch_ascend(dpop, static_cast<ce_node_gene*>(a->d_nodes.ptr),
+                                    static_cast<ce_muscle_gene*>(a->d_muscle_genes.ptr),
+                                    a->has_strength ? static_cast<float*>(a->d_strength.ptr) : nullptr,
+                                    static_cast<const double*>(a->d_mg.ptr), static_cast<const double*>(a->d_ng.ptr),
+                                    step_size, st);
+        if (ce == cudaSuccess)
+            ce = cek::launch_pack(dpop, static_cast<const float*>(a->d_trig.ptr),
+                                  static_cast<const uint32_t*>(a->d_order.ptr),
+                                  static_cast<const uint32_t*>(a->d_rat.ptr), static_cast<const uint32_t*>(a->d_mat.ptr),
+                                  n, a->world, static_cast<uint32_t*>(a->d_lanes.ptr),
+                                  static_cast<float*>(a->d_muscles.ptr), static_cast<uint32_t*>(a->d_heads.ptr), st);
+    }
+    if (ce == cudaSuccess) ce = cek::launch_bucket(heads_d, 0u, (uint32_t)n, bk, st);
+    if (ce == cudaSuccess) {
+        cek::KernelArgs ka = args(steps);
+        ka.ckpt = nullptr;
+        ka.ends = nullptr;
+        const cek::LaunchSpec ls{a->rows, a->mm, flags, false, a->rate, fgrid, cek::kBlock, st};
+        ce = cek::launch_advance(ls, ka, a->params);
+    }
+    cudaGraph_t graph = nullptr;
+    const ce_status end = cuda_status(cudaStreamEndCapture(st, &graph), "cudaStreamEndCapture");
+    a->graph = graph;
+    if ((s = cuda_status(ce, "ascent capture")) != CE_OK) return fail(s);
+    if (end != CE_OK) return fail(end);
+    if ((s = cuda_status(cudaGraphInstantiate(&a->exec, a->graph, 0), "cudaGraphInstantiate")) != CE_OK) return fail(s);
+    *out = a;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_ascent_launch(ce_ascent* a, double* seconds) {
+    if (!a || !a->exec) return CE_ERR_INVALID;
+    ce_status s = set_device(a->engine);
+    if (s != CE_OK) return s;
+    CE_TRY(cudaEventRecord(a->start, a->stream), "cudaEventRecord");
+    CE_TRY(cudaGraphLaunch(a->exec, a->stream), "cudaGraphLaunch");
+    CE_TRY(cudaEventRecord(a->stop, a->stream), "cudaEventRecord");
+    CE_TRY(cudaEventSynchronize(a->stop), "ascent graph");
+    float ms = 0.0f;
+    CE_TRY(cudaEventElapsedTime(&ms, a->start, a->stop), "cudaEventElapsedTime");
+    if (seconds) *seconds = ms * 1e-3;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_ascent_fitness(ce_ascent* a, uint32_t step, float* fitness, size_t cap) {
+    if (!a || !fitness || step > a->steps || cap < a->count) {
+        set_error("ce_ascent_fitness: bad step or buffer too small");
+        return CE_ERR_INVALID;
+    }
+    ce_status s = set_device(a->engine);
+    if (s != CE_OK) return s;
+    std::vector<ce_result> res(a->count);
+    CE_TRY(cudaMemcpy(res.data(), a->d_results[step].ptr, a->count * sizeof(ce_result), cudaMemcpyDeviceToHost),
+           "cudaMemcpy");
+    for (size_t c = 0; c < a->count; c++) fitness[a->order[c]] = res[c].fitness;
+    return CE_OK;
+}
+
+extern "C" ce_status ce_ascent_genes(ce_ascent* a, ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength) {
+    if (!a || !nodes || !muscles) return CE_ERR_INVALID;
+    ce_status s = set_device(a->engine);
+    if (s != CE_OK) return s;
+    CE_TRY(cudaMemcpy(nodes, a->d_nodes.ptr, a->nodes_len * sizeof(ce_node_gene), cudaMemcpyDeviceToHost),
+           "cudaMemcpy");
+    CE_TRY(cudaMemcpy(muscles, a->d_muscle_genes.ptr, a->muscles_len * sizeof(ce_muscle_gene),
+                      cudaMemcpyDeviceToHost),
+           "cudaMemcpy");
+    if (strength && a->has_strength) {
+        CE_TRY(cudaMemcpy(strength, a->d_strength.ptr, a->muscles_len * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    }
+    return CE_OK;
+}
+
 // ------------------------------------------------------ generation graphs
 // Several packed generations run as one CUDA graph: per generation the
 // node-count bucketing and the size classes' launches (two streams joined

@@ -130,6 +130,15 @@ struct LaunchSpec {
 unsigned slot_lines(unsigned rows, unsigned mm, bool record);
 
 cudaError_t launch_advance(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
+// The device packer and the refinement's ascent (csrc/pack.cu).
+cudaError_t launch_pack(const ce_population& pop, const float* trig, const uint32_t* order, const uint32_t* record_at,
+                        const uint32_t* muscle_at, size_t n, const ce_world& w, uint32_t* lanes, float* muscles,
+                        uint32_t* heads, cudaStream_t stream);
+cudaError_t launch_gene_grads(const ce_population& pop, const float* trig, const uint32_t* order, size_t n,
+                              const ce_world& w, const float* grads, uint32_t rows, uint32_t mm, double* muscle_grads,
+                              double* node_grads, cudaStream_t stream);
+cudaError_t launch_ascend(const ce_population& pop, ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength,
+                          const double* muscle_grads, const double* node_grads, double step, cudaStream_t stream);
 // A recording's frames from the kernel's frame-major, creature-minor layout
 // (`rows` = frames x slots rows of `creatures` entries) to the reference's
 // creature-major one (`creatures` rows of `rows` entries).

@@ -70,3 +70,111 @@ extern "C" ce_status ce_pack_device(const ce_population* pop, const float* trig,
     }
     return CE_OK;
 }
+
+// ------------------------------------------------- the refinement's ascent
+// Gene gradients on the device (the host's ce_gene_gradients, the same
+// double arithmetic: packer.h), one creature a thread, from the backward
+// run's record gradients of the packed batch.
+namespace {
+
+__global__ void __launch_bounds__(128) gene_grads_kernel(const ce_population pop, const float* trig,
+                                                         const uint32_t* order, size_t n, const ce_world w,
+                                                         const float* grads, uint32_t rows, uint32_t mm,
+                                                         double* muscle_grads, double* node_grads) {
+    const size_t per = (size_t)9 * mm + 4 * (size_t)rows;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t i = order[c];
+        const float* t = trig + 3 * (size_t)pop.genomes[i].bone_start;
+        ce::gene_gradients_one(pop, i, w, grads + c * per, rows, mm, muscle_grads, node_grads, PlanAngle{t},
+                               PlanTrig{t});
+    }
+}
+
+__device__ __forceinline__ double finite_or_zero(double g) { return isfinite(g) ? g : 0.0; }
+// step x g clipped to [-unit, unit], rounded to float (g finite: a NaN or
+// infinite gradient counts as 0).
+__device__ __forceinline__ float clipped_move(double step, double g, double unit) {
+    double v = step * g;
+    v = v < -unit ? -unit : v;
+    v = v > unit ? unit : v;
+    return (float)v;
+}
+__device__ __forceinline__ float clip32(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+// x mod 1 into [0, 1), as numpy's float32 remainder rounds it.
+__device__ __forceinline__ float wrap_unit(float x) {
+    float m = fmodf(x, 1.0f);
+    if (m != 0.0f) {
+        if (m < 0.0f) m += 1.0f;
+    } else {
+        m = 0.0f;
+    }
+    return m;
+}
+
+// One clipped ascent step of every creature's differentiated genes, in
+// place: per muscle short, long, strength scale, phase and duty, per node
+// friction; each move is step x gradient clipped to the coordinate's unit
+// (0.02 x the body's mean bone length for lengths, 0.05 for phase, duty
+// and strength, 0.03 for friction), then the genes' clamps.
+__global__ void __launch_bounds__(128) ascend_kernel(const ce_genome* genomes, const ce_bone_gene* bones,
+                                                     ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength,
+                                                     const double* muscle_grads, const double* node_grads,
+                                                     size_t count, double step) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        const ce_genome g = genomes[i];
+        double total = 0.0;
+        for (uint32_t j = 0; j < g.bone_count; j++) total += (double)bones[g.bone_start + j].rest_length;
+        double size = g.bone_count > 0 ? total / (double)g.bone_count : 1.0;
+        size = size < 0.05 ? 0.05 : (size > 10.0 ? 10.0 : size);
+        const double unit = (double)(0.02f * (float)size);
+        for (uint32_t k = 0; k < g.muscle_count; k++) {
+            ce_muscle_gene& m = muscles[g.muscle_start + k];
+            const double* d = muscle_grads + 5 * (size_t)(g.muscle_start + k);
+            const double T = (double)m.period;
+            const float s = clip32(m.short_len + clipped_move(step, finite_or_zero(d[0]), unit), 0.01f, 1.6f);
+            m.short_len = s;
+            m.long_len = clip32(m.long_len + clipped_move(step, finite_or_zero(d[1]), unit), s, 2.0f);
+            m.phase = wrap_unit(m.phase + clipped_move(step, -T * (finite_or_zero(d[3]) + finite_or_zero(d[4])), 0.05));
+            m.duty = clip32(m.duty + clipped_move(step, T * finite_or_zero(d[4]), 0.05), 0.05f, 0.95f);
+            if (strength) {
+                float& st = strength[g.muscle_start + k];
+                st = clip32(st + clipped_move(step, finite_or_zero(d[2]), 0.05), 0.5f, 1.5f);
+            }
+        }
+        for (uint32_t r = 0; r < g.node_count; r++) {
+            ce_node_gene& nd = nodes[g.node_start + r];
+            nd.friction = clip32(nd.friction + clipped_move(step, finite_or_zero(node_grads[g.node_start + r]), 0.03), 0.0f, 1.0f);
+        }
+    }
+}
+
+}  // namespace
+
+namespace cek {
+cudaError_t launch_gene_grads(const ce_population& pop, const float* trig, const uint32_t* order, size_t n,
+                              const ce_world& w, const float* grads, uint32_t rows, uint32_t mm, double* muscle_grads,
+                              double* node_grads, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const size_t blocks = (n + 127) / 128;
+    gene_grads_kernel<<<(unsigned)(blocks < 148u * 32u ? blocks : 148u * 32u), 128, 0, stream>>>(
+        pop, trig, order, n, w, grads, rows, mm, muscle_grads, node_grads);
+    return cudaGetLastError();
+}
+cudaError_t launch_ascend(const ce_population& pop, ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength,
+                          const double* muscle_grads, const double* node_grads, double step, cudaStream_t stream) {
+    if (pop.count == 0) return cudaSuccess;
+    const size_t blocks = (pop.count + 127) / 128;
+    ascend_kernel<<<(unsigned)(blocks < 148u * 32u ? blocks : 148u * 32u), 128, 0, stream>>>(
+        pop.genomes, pop.bones, nodes, muscles, strength, muscle_grads, node_grads, pop.count, step);
+    return cudaGetLastError();
+}
+cudaError_t launch_pack(const ce_population& pop, const float* trig, const uint32_t* order, const uint32_t* record_at,
+                        const uint32_t* muscle_at, size_t n, const ce_world& w, uint32_t* lanes, float* muscles,
+                        uint32_t* heads, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const size_t blocks = (n + 127) / 128;
+    pack_kernel<<<(unsigned)(blocks < 148u * 32u ? blocks : 148u * 32u), 128, 0, stream>>>(
+        pop, trig, order, record_at, muscle_at, n, w, lanes, muscles, heads);
+    return cudaGetLastError();
+}
+}  // namespace cek
