@@ -254,7 +254,7 @@ def _evaluate(engine, pop, world, chunk: int):
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
            resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None,
-           sampler: str = "host", guided: bool = False) -> dict:
+           sampler: str = "host", guided: bool = False, ascent: str = "device") -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -276,10 +276,14 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     (samples_gpu), "host" with numpy (samples). With `guided`, a third arm
     spends the same GPU time on one gradient of each elite (the
     refinement's first forward and backward run) and children drawn around
-    the elite moved by one ascent step instead of around the elite."""
+    the elite moved by one ascent step instead of around the elite.
+    `ascent` "device" runs the ascent steps and the last scoring as one CUDA
+    graph on the GPU (api.Ascent: no host round trip between the steps),
+    "host" step by step through the host (packing, gene gradients and the
+    step in numpy); both give the same fitness and genes."""
     draw = samples if sampler == "host" else samples_gpu
     report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
-                  ranks=world_size, sampler=sampler)
+                  ranks=world_size, sampler=sampler, ascent=ascent)
     lo, hi = count * rank // world_size, count * (rank + 1) // world_size
     t0 = time.perf_counter()
     base = api.generate(spec, parents)
@@ -299,27 +303,43 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     first_equal = True
     stepped, grad_s = None, 0.0
     t0 = time.perf_counter()
-    for k in range(steps if len(mine) else 0):
-        wave = api.pack(x, world)
-        with engine.forward(wave, world) as tape:
-            fk = _fitness(wave, tape.results).astype(np.float64)
-            g = tape.backward()
-            shape = tape.shape
-            fwd, bwd = tape.seconds
-        refine_s += fwd + bwd
-        if k == 0:
-            # The elites' genes, scored again by the checkpointed forward run.
-            first_equal = bool(np.array_equal(fk, f0))
-        best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
-        mg, ng = api.gene_gradients(x, wave, world, g, shape)
-        x = ascend(x, mg, ng, step)
-        if k == 0:
-            stepped, grad_s = x, fwd + bwd
     last_s = 0.0
-    if len(mine):
-        fk, last_s = _evaluate(engine, x, world, chunk)
-        refine_s += last_s
-        best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+    if ascent == "device" and len(mine) and steps:
+        with api.Ascent(engine, elite, world, steps, step) as asc:
+            refine_s = asc.launch()
+            for k in range(steps + 1):
+                fk = asc.fitness(k).astype(np.float64)
+                if k == 0:
+                    first_equal = bool(np.array_equal(fk, f0))
+                best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+        if guided:
+            # The genes after one step, and that step's GPU time (a
+            # one-step ascent: its forward and backward runs, the step and
+            # one scoring of the moved genes).
+            with api.Ascent(engine, elite, world, 1, step) as one:
+                grad_s = one.launch()
+                stepped = one.population()
+    else:
+        for k in range(steps if len(mine) else 0):
+            wave = api.pack(x, world)
+            with engine.forward(wave, world) as tape:
+                fk = _fitness(wave, tape.results).astype(np.float64)
+                g = tape.backward()
+                shape = tape.shape
+                fwd, bwd = tape.seconds
+            refine_s += fwd + bwd
+            if k == 0:
+                # The elites' genes, scored again by the checkpointed forward run.
+                first_equal = bool(np.array_equal(fk, f0))
+            best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
+            mg, ng = api.gene_gradients(x, wave, world, g, shape)
+            x = ascend(x, mg, ng, step)
+            if k == 0:
+                stepped, grad_s = x, fwd + bwd
+        if len(mine):
+            fk, last_s = _evaluate(engine, x, world, chunk)
+            refine_s += last_s
+            best = np.maximum(best, np.where(fk > -1e19, fk, -np.inf))
     host_refine = time.perf_counter() - t0
     tot = shard.all_sum([len(mine), f0.sum(), best.sum(), (best > f0).sum(), busy, refine_s,
                          0.0 if first_equal else 1.0, last_s], world_size, group, device)

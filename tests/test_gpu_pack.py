@@ -61,8 +61,9 @@ def test_device_packing_equals_host_packing(name, count, strength):
     plan, lanes, muscles, heads = device_pack(pop, world)
     assert (plan.order == wave.slots).all()
     assert len(lanes) == len(wave.lanes) and len(muscles) == len(wave.muscles)
-    bad = np.nonzero(heads != wave.heads)[0]
-    assert len(bad) == 0, f"{len(np.unique(bad))} heads differ, first {bad[:4]}"
+    rows, cols = np.nonzero(heads != wave.heads)
+    assert len(rows) == 0, (f"{len(np.unique(rows))} heads differ in words {np.unique(cols)}; first "
+                            f"{rows[:2]}: device {heads[rows[0]]} host {wave.heads[rows[0]]}")
     bad = np.nonzero(lanes != wave.lanes)[0]
     assert len(bad) == 0, f"{len(bad)} record words differ, first at {bad[:4]}"
     bad = np.nonzero(muscles != wave.muscles.view(np.uint32))[0]

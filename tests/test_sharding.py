@@ -145,7 +145,7 @@ def search_worker(rank, world_size, port, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world_size)
     try:
         w = WORKLOADS["refine"]
-        rep = refine.search(OracleEngine(), w.spec, w.world(duration=0.5), parents=16, count=600, elites=40, steps=1,
+        rep = refine.search(OracleEngine(), w.spec, w.world(duration=0.5), parents=16, count=600, elites=40, steps=1, ascent="host",
                             resample=False, rank=rank, world_size=world_size)
         np.save(os.path.join(out_dir, f"rep{rank}.npy"),
                 np.array([rep["elite_mean_fitness"], rep["refine"]["mean_best"], rep["sample_gpu_s"],
@@ -162,7 +162,7 @@ def test_refined_search_splits_over_two_ranks(tmp_path):
     port = free_port()
     mp.start_processes(search_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
     w = WORKLOADS["refine"]
-    one = refine.search(OracleEngine(), w.spec, w.world(duration=0.5), parents=16, count=600, elites=40, steps=1,
+    one = refine.search(OracleEngine(), w.spec, w.world(duration=0.5), parents=16, count=600, elites=40, steps=1, ascent="host",
                         resample=False)
     for r in range(2):
         got = np.load(tmp_path / f"rep{r}.npy")
