@@ -218,29 +218,6 @@ ce_status ce_pack_device(const ce_population* pop, const float* trig, const uint
                          const uint32_t* record_at, const uint32_t* muscle_at, size_t n, const ce_world* world,
                          uint32_t* lanes, float* muscles, uint32_t* heads, void* stream);
 
-/* A batch's gradient ascent kept on the device, as one CUDA graph (no
- * counterpart in the reference, which refines only by CMA-ES). Opening packs
- * the `pop->count` creatures once on the host (the plan of ce_pack_plan),
- * uploads their genes (arrays of nodes_len, bones_len, muscles_len genes;
- * the strength scale if given) and captures `steps` ascent steps and a last
- * scoring: per step the checkpointed forward run (scoring the step's
- * genes), the backward run of d(sum of fitness), the gene gradients (as
- * ce_gene_gradients), one clipped ascent step of `step_size` on each muscle's
- * short, long, strength scale, phase and duty and each node's friction
- * (each move clipped to the coordinate's unit: 0.02 x the body's mean bone
- * length, 0.05, 0.03 for friction; then the genes' clamps) and the
- * repacking of the records on the device (ce_pack_device). The calm and
- * effects worlds, no touch sensors. ce_ascent_launch runs the graph;
- * ce_ascent_fitness gives step k's fitness in population order (k = steps:
- * the last genes); ce_ascent_genes copies the genes back. */
-typedef struct ce_ascent ce_ascent;
-ce_status ce_ascent_open(ce_engine* engine, const ce_population* pop, const ce_world* world, uint32_t steps,
-                         double step_size, size_t nodes_len, size_t bones_len, size_t muscles_len, ce_ascent** out);
-ce_status ce_ascent_launch(ce_ascent* ascent, double* seconds);
-ce_status ce_ascent_fitness(ce_ascent* ascent, uint32_t step, float* fitness, size_t cap);
-ce_status ce_ascent_genes(ce_ascent* ascent, ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength);
-ce_status ce_ascent_close(ce_ascent* ascent);
-
 /* The ground's height and slope under x for bump height `amplitude`, slope
  * `tilt`, pit width `width`, hurdle height `hurdle` and quake phase `phase`
  * (physics::ground, src/physics.rs:668-683), as the packer places creatures
@@ -553,6 +530,29 @@ ce_status ce_measure_fp32(int device, double* tflops, double* seconds);
 /* Host-side fault injection for the recovery paths (src/scheduler.rs:725):
  * the `after`-th next submit fails with `status`. 0 turns it off. */
 ce_status ce_inject_fault(ce_engine* engine, uint32_t after, ce_status status);
+
+/* A batch's gradient ascent kept on the device, as one CUDA graph (no
+ * counterpart in the reference, which refines only by CMA-ES). Opening packs
+ * the `pop->count` creatures once on the host (the plan of ce_pack_plan),
+ * uploads their genes (arrays of nodes_len, bones_len, muscles_len genes;
+ * the strength scale if given) and captures `steps` ascent steps and a last
+ * scoring: per step the checkpointed forward run (scoring the step's
+ * genes), the backward run of d(sum of fitness), the gene gradients (as
+ * ce_gene_gradients), one clipped ascent step of `step_size` on each muscle's
+ * short, long, strength scale, phase and duty and each node's friction
+ * (each move clipped to the coordinate's unit: 0.02 x the body's mean bone
+ * length, 0.05, 0.03 for friction; then the genes' clamps) and the
+ * repacking of the records on the device (ce_pack_device). The calm and
+ * effects worlds, no touch sensors. ce_ascent_launch runs the graph;
+ * ce_ascent_fitness gives step k's fitness in population order (k = steps:
+ * the last genes); ce_ascent_genes copies the genes back. */
+typedef struct ce_ascent ce_ascent;
+ce_status ce_ascent_open(ce_engine* engine, const ce_population* pop, const ce_world* world, uint32_t steps,
+                         double step_size, size_t nodes_len, size_t bones_len, size_t muscles_len, ce_ascent** out);
+ce_status ce_ascent_launch(ce_ascent* ascent, double* seconds);
+ce_status ce_ascent_fitness(ce_ascent* ascent, uint32_t step, float* fitness, size_t cap);
+ce_status ce_ascent_genes(ce_ascent* ascent, ce_node_gene* nodes, ce_muscle_gene* muscles, float* strength);
+ce_status ce_ascent_close(ce_ascent* ascent);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,23 @@ def test_library_exports_every_declared_function():
     assert set(api.EXPORTED) <= set(names)
 
 
+def test_header_compiles_as_c11_and_cpp17(tmp_path):
+    """The header is what a cgo / ctypes / JNI binding includes: it must
+    stand alone in C and C++ (every type declared before its first use)."""
+    import shutil
+    import subprocess
+    src = tmp_path / "use.c"
+    src.write_text('#include "creature_engine.h"\nint main(void) { return 0; }\n')
+    for tool, std in (("gcc", "-std=c11"), ("g++", "-std=c++17")):
+        if shutil.which(tool) is None:
+            continue
+        cmd = [tool, std, "-Wall", "-Werror", "-fsyntax-only", "-I", str(HEADER.parent)]
+        if tool == "g++":
+            cmd += ["-x", "c++"]
+        proc = subprocess.run(cmd + [str(src)], capture_output=True, text=True)
+        assert proc.returncode == 0, proc.stderr[-2000:]
+
+
 def test_struct_layouts():
     # Params: 25 words and two rungs of 8 (shaders/creature.cu:66-103).
     assert C.sizeof(api.Params) == 25 * 4 + 2 * 32
