@@ -28,6 +28,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--prec-div=false", "--prec-sqrt=false", "--fmad=true",
     "-extra-device-vectorization", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
+    # A host-only function called from device code has no device body: an
+    # error, not a warning (the call would be undefined on the GPU).
+    "-Werror", "cross-execution-space-call",
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp"]
 

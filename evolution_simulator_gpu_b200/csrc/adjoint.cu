@@ -240,13 +240,14 @@ struct Backward {
 
     __device__ __forceinline__ void load_checkpoint(unsigned s) const {
         const LaneRegs& r = b.r;
-        const float* c = a.ckpt + (size_t)r.cidx * a.ckpt_stride + (size_t)s * checkpoint_floats(a.rows, a.mm);
+        const size_t n = a.count;
+        const float* c = a.ckpt + (size_t)s * checkpoint_floats(a.rows, a.mm) * n + r.cidx;
         for (unsigned i = 0u; i < r.nodes; i++) {
-            b.t.pos(i) = make_float2(c[2u * i], c[2u * i + 1u]);
-            b.t.vel(i) = make_float2(c[2u * a.rows + 2u * i], c[2u * a.rows + 2u * i + 1u]);
+            b.t.pos(i) = make_float2(c[(2u * i) * n], c[(2u * i + 1u) * n]);
+            b.t.vel(i) = make_float2(c[(2u * a.rows + 2u * i) * n], c[(2u * a.rows + 2u * i + 1u) * n]);
         }
         for (unsigned m = 0u; m < r.muscles; m++) {
-            b.t.muscle(m).x = c[4u * a.rows + m];
+            b.t.muscle(m).x = c[(4u * a.rows + m) * n];
         }
     }
 

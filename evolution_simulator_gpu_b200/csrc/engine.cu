@@ -777,7 +777,6 @@ cek::KernelArgs tape_args(ce_tape* t, const cek::Buckets& bk) {
     a.mm = t->mm;
     a.chunk_k = t->engine->chunk_k;
     a.ckpt = static_cast<float*>(t->d_ckpt.ptr);
-    a.ckpt_stride = t->ckpts * cek::checkpoint_floats(t->rows, t->mm);
     a.ends = static_cast<uint32_t*>(t->d_ends.ptr);
     return a;
 }
@@ -984,7 +983,13 @@ extern "C" ce_status ce_tape_checkpoints(ce_tape* t, float* out, size_t cap_floa
     }
     ce_status s = set_device(t->engine);
     if (s != CE_OK) return s;
-    CE_TRY(cudaMemcpy(out, t->d_ckpt.ptr, per * t->count * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    // The device keeps them creature-minor ([checkpoint][float][creature]);
+    // the caller gets [creature][checkpoint][float].
+    std::vector<float> stage(per * t->count);
+    CE_TRY(cudaMemcpy(stage.data(), t->d_ckpt.ptr, per * t->count * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (size_t c = 0; c < t->count; c++) {
+        for (size_t f = 0; f < per; f++) out[c * per + f] = stage[f * t->count + c];
+    }
     if (per_creature) *per_creature = t->ckpts;
     return CE_OK;
 }
@@ -1163,7 +1168,6 @@ extern "C" ce_status ce_ascent_open(ce_engine* e, const ce_population* pop, cons
         k.mm = a->mm;
         k.chunk_k = e->chunk_k;
         k.ckpt = static_cast<float*>(a->d_ckpt.ptr);
-        k.ckpt_stride = a->ckpts * cek::checkpoint_floats(a->rows, a->mm);
         k.ends = static_cast<uint32_t*>(a->d_ends.ptr);
         return k;
     };

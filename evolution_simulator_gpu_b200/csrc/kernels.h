@@ -58,8 +58,8 @@ struct KernelArgs {
     uint32_t mm;                   // most muscles of a body of this launch
     uint32_t frames_per_creature;  // RECORD: frames of one recording
     uint32_t chunk_k;              // claims shrink to 1 / chunk_k of the rest per warp
-    float* ckpt;                   // CKPT: checkpoints, ckpt_stride floats a creature (packed index)
-    uint32_t ckpt_stride;
+    float* ckpt;                   // CKPT: checkpoints, creature-minor: float f of checkpoint k of
+                                   // creature c (packed index) at (k * checkpoint_floats + f) * count + c
     uint32_t* ends;                // CKPT: steps each creature's trial ran (packed index)
     // Niche epilogue at the result store (plain kernel; `cells` NULL: none):
     // each creature's metrics row (`metrics` may be NULL) and dense cell,

@@ -365,7 +365,7 @@ CE_HD Model make_model(const ce_node_gene* g, size_t n, const ce_bone_gene* bone
     struct Key {
         uint32_t lo, hi;
         bool side;
-        bool operator==(const Key& o) const { return lo == o.lo && hi == o.hi && side == o.side; }
+        CE_HD bool operator==(const Key& o) const { return lo == o.lo && hi == o.hi && side == o.side; }
     };
     auto bone_point = [&](const ce_bone_gene& b, float t, float out[2]) {
         const ce_node_gene& a = g[b.a];

@@ -42,18 +42,21 @@ struct Trial {
 
     // Checkpoint `k` of the creature (the state at substep 256 k): positions,
     // velocities and energy stores, the whole state that the substeps carry
-    // from one step to the next in a world without touch sensors.
+    // from one step to the next in a world without touch sensors. Stored
+    // creature-minor, so that the lanes of a warp (creatures claimed in
+    // packed order) write neighbouring words.
     __device__ __forceinline__ static void save_checkpoint(const Body& b, const KernelArgs& a, unsigned k) {
-        float* c = a.ckpt + (size_t)b.r.cidx * a.ckpt_stride + (size_t)k * checkpoint_floats(a.rows, a.mm);
+        const size_t n = a.count;
+        float* c = a.ckpt + (size_t)k * checkpoint_floats(a.rows, a.mm) * n + b.r.cidx;
         for (unsigned i = 0u; i < b.r.nodes; i++) {
             const float2 q = b.t.pos(i), v = b.t.vel(i);
-            c[2u * i] = q.x;
-            c[2u * i + 1u] = q.y;
-            c[2u * a.rows + 2u * i] = v.x;
-            c[2u * a.rows + 2u * i + 1u] = v.y;
+            __stcs(c + (2u * i) * n, q.x);
+            __stcs(c + (2u * i + 1u) * n, q.y);
+            __stcs(c + (2u * a.rows + 2u * i) * n, v.x);
+            __stcs(c + (2u * a.rows + 2u * i + 1u) * n, v.y);
         }
         for (unsigned k2 = 0u; k2 < b.r.muscles; k2++) {
-            c[4u * a.rows + k2] = b.t.muscle(k2).x;
+            __stcs(c + (4u * a.rows + k2) * n, b.t.muscle(k2).x);
         }
     }
 

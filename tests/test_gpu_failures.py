@@ -49,7 +49,7 @@ def test_injected_fault_fails_one_submission_then_the_engine_recovers(batch, sta
         with pytest.raises(ce.EngineError) as err:
             eng.submit(wave, world)
         assert err.value.status == status
-        assert err.value.out_of_memory() == (status == ce.CE_ERR_OOM)
+        assert err.value.out_of_memory == (status == ce.CE_ERR_OOM)
         assert b"injected" in ce.lib().ce_last_error()
         got = eng.poll(600.0)
         assert got is not None and got[0] == t1

@@ -240,3 +240,32 @@ def test_gradients_refuse_unsupported_batches(engine):
     with pytest.raises(ce.EngineError) as err:
         engine.forward(wave, world)
     assert err.value.status == ce.CE_ERR_UNSUPPORTED
+
+
+def test_checkpoints_hold_the_state_every_16_steps(engine):
+    """The forward run's checkpoints (stored creature-minor on the device,
+    returned per creature): checkpoint 0 is the packed start pose at rest
+    with full energy stores, and the positions of checkpoint 2 (after 32
+    steps) put the centre of mass where a 32-step trial of the plain kernel
+    ends (its fitness)."""
+    world = W.world(duration=1.0)
+    wave = ce.pack(ce.generate(W.spec, 1024), world)
+    with engine.forward(wave, world) as tape:
+        ck = tape.checkpoints(ce.trial_steps(world))
+        rows, mm = tape.shape
+    short = W.world(duration=32.0 / 60.0)
+    assert ce.trial_steps(short) == 32
+    res, _ = engine.run(wave, short)
+    lf = wave.lanes.view(np.float32)
+    com = np.zeros(len(wave))
+    for c in range(len(wave)):
+        n, m, ro = int(wave.heads[c, 0] & 255), int(wave.heads[c, 1]), int(wave.heads[c, 3])
+        start = np.stack([lf[ro + 6 * np.arange(n) + 3], lf[ro + 6 * np.arange(n) + 4]], axis=1).reshape(-1)
+        assert (ck[c, 0, :2 * n] == start).all(), c
+        assert (ck[c, 0, 2 * rows:2 * rows + 2 * n] == 0).all(), c
+        assert (ck[c, 0, 4 * rows:4 * rows + m] == 1).all(), c
+        mass = lf[ro + 6 * np.arange(n)].astype(np.float64)
+        com[c] = (mass * ck[c, 2, 0:2 * n:2]).sum() / mass.sum()
+    ok = (res["fall_time"] == 0) & (res["fitness"] > -1e19)
+    assert ok.mean() > 0.9
+    assert np.allclose(com[ok], res["fitness"][ok], rtol=1e-5, atol=1e-5)
