@@ -218,6 +218,7 @@ def _bind(lib: C.CDLL) -> None:
         "ce_tape_seconds": (C.c_int, [C.c_void_p, P(C.c_double), P(C.c_double)]),
         "ce_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
         "ce_tape_free": (C.c_int, [C.c_void_p]),
+        "ce_tangent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
         "ce_tape_checkpoints": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(C.c_uint32)]),
         "ce_gene_gradients": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_void_p, C.c_void_p,
                                         C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -246,7 +247,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_ascent_fitness", "ce_ascent_genes", "ce_ascent_close", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
-            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_gene_gradients", "ce_tape_checkpoints",
+            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_tangent", "ce_gene_gradients", "ce_tape_checkpoints",
             "ce_replay_decode", "ce_sample_rows", "ce_sample_device", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
             "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
 
@@ -834,6 +835,18 @@ class Tape:
         if w is not None and len(w) != self.count:
             raise ValueError("one weight a creature")
         _check(lib().ce_backward(self._handle(), _ptr(w), _ptr(out), out.size), "ce_backward")
+        return out
+
+    def tangent(self, dstart) -> np.ndarray:
+        """d fitness of each creature along a direction of its start
+        positions (`dstart` [creature, rows, 2] in packed order, as the
+        start-position part of `backward`'s rows), by the tangent-linear run
+        on the forward run's FP32 trajectory (calm world): the adjoint's
+        check, <backward start gradient, dstart> = tangent."""
+        rows, _ = self.shape
+        d = np.ascontiguousarray(dstart, np.float32).reshape(self.count, rows * 2)
+        out = np.zeros(self.count, np.float32)
+        _check(lib().ce_tangent(self._handle(), _ptr(d), d.size, _ptr(out)), "ce_tangent")
         return out
 
     def checkpoints(self, steps: int) -> np.ndarray:

@@ -96,6 +96,14 @@ bool gradient_world(uint32_t flags);
 cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, uint32_t flags, int rate, int* blocks);
 struct LaunchSpec;
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
+// The tangent-linear run (the adjoint's check; calm world only): d fitness
+// of each creature along start-position tangents dstart (2 x rows floats a
+// creature, packed index) into dfitness, on the lane slots of
+// adjoint_slot_bytes and the checkpointed forward run's ends and results.
+size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block);
+bool tangent_world(uint32_t flags);
+cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
+                           float* dfitness);
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
                            const float* weights);
 

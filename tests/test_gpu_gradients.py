@@ -266,6 +266,8 @@ def test_checkpoints_hold_the_state_every_16_steps(engine):
         assert (ck[c, 0, 4 * rows:4 * rows + m] == 1).all(), c
         mass = lf[ro + 6 * np.arange(n)].astype(np.float64)
         com[c] = (mass * ck[c, 2, 0:2 * n:2]).sum() / mass.sum()
+    # Bodies that fall within the 32 steps (about a third, toppling as they
+    # settle) end their trial before checkpoint 2.
     ok = (res["fall_time"] == 0) & (res["fitness"] > -1e19)
-    assert ok.mean() > 0.9
+    assert ok.sum() >= 256, ok.sum()
     assert np.allclose(com[ok], res["fitness"][ok], rtol=1e-5, atol=1e-5)
