@@ -216,25 +216,29 @@ struct Backward {
         }
     }
 
+    // The segment tape streams through L2 (2.2 MB a warp at 12 node rows and
+    // 20 muscle slots, each substep's state written once and read back by
+    // the reverse pass up to 255 substeps later), so its stores and loads
+    // carry the evict-first hint and leave L2 to the lane slots.
     __device__ __forceinline__ void load_state(unsigned k) const {
         const LaneRegs& r = b.r;
         for (unsigned i = 0u; i < r.nodes; i++) {
-            b.t.pos(i) = *tape.pair(k, 2u * i);
-            b.t.vel(i) = *tape.pair(k, 2u * a.rows + 2u * i);
+            b.t.pos(i) = __ldcs(tape.pair(k, 2u * i));
+            b.t.vel(i) = __ldcs(tape.pair(k, 2u * a.rows + 2u * i));
         }
         for (unsigned m = 0u; m < r.muscles; m++) {
-            b.t.muscle(m).x = *tape.word(k, 4u * a.rows + m);
+            b.t.muscle(m).x = __ldcs(tape.word(k, 4u * a.rows + m));
         }
     }
 
     __device__ __forceinline__ void save_state(unsigned k) const {
         const LaneRegs& r = b.r;
         for (unsigned i = 0u; i < r.nodes; i++) {
-            *tape.pair(k, 2u * i) = b.t.pos(i);
-            *tape.pair(k, 2u * a.rows + 2u * i) = b.t.vel(i);
+            __stcs(tape.pair(k, 2u * i), b.t.pos(i));
+            __stcs(tape.pair(k, 2u * a.rows + 2u * i), b.t.vel(i));
         }
         for (unsigned m = 0u; m < r.muscles; m++) {
-            *tape.word(k, 4u * a.rows + m) = b.t.muscle(m).x;
+            __stcs(tape.word(k, 4u * a.rows + m), b.t.muscle(m).x);
         }
     }
 
@@ -827,7 +831,10 @@ struct Backward {
         const float c = kMuscleRecovery * p.muscle_recovery * C::h;
         for (unsigned k = 0u; k < r.muscles; k++) {
             const unsigned m0 = S.muscle + 5u * k;
-            const float4 q0 = L.get(m0 + kPull0), q1 = L.get(m0 + kPull1);
+            const float4 q0 = L.get(m0 + kPull0);
+            const float2 qc = L.get2(S.cap, k);
+            const float2 qt = r.tendon ? L.get2(S.tendon, k) : make_float2(0.0f, 0.0f);
+            const float4 q1 = make_float4(qc.x, qc.y, qt.x, qt.y);
             const float2 ms = t.muscle(k);
             const unsigned nodes = __float_as_uint(q0.x);
             const unsigned a0 = nodes & 255u, a1 = (nodes >> 8u) & 255u, b0 = (nodes >> 16u) & 255u,

@@ -271,3 +271,43 @@ def test_checkpoints_hold_the_state_every_16_steps(engine):
     ok = (res["fall_time"] == 0) & (res["fitness"] > -1e19)
     assert ok.sum() >= 256, ok.sum()
     assert np.allclose(com[ok], res["fitness"][ok], rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("seconds", [16.0 / 60.0, 20.0])
+def test_adjoint_equals_the_tangent_linear_run(engine, seconds):
+    """The dot-product test of the adjoint: for a random direction u of the
+    start positions, <backward's start gradient, u> against the tangent-linear
+    run (ce_tangent) along u. Both differentiate the forward run's own FP32
+    trajectory with its contact, slip and joint-limit modes, so they differ
+    only by the rounding of the two FP32 derivative computations (the FP64
+    tangent of the oracle takes its own modes). Config 4: 256 creatures of
+    seed 3 in the calm world, over one 16-step segment and over 20 s, where
+    the derivatives reach 1e30 on near-degenerate joints."""
+    world = W.world(duration=seconds)
+    wave = ce.pack(ce.generate(W.spec, 256), world)
+    with engine.forward(wave, world) as tape:
+        rows, mm = tape.shape
+        g = tape.backward()
+        res = tape.results
+        ds = np.random.default_rng(11).normal(size=(len(wave), rows, 2)).astype(np.float32)
+        for c in range(len(wave)):
+            ds[c, int(wave.heads[c, 0] & 255):] = 0
+        tan = tape.tangent(ds)
+    start = g[:, 9 * mm + 2 * rows:9 * mm + 4 * rows].astype(np.float64)
+    adj = (start * ds.reshape(len(wave), -1)).sum(axis=1)
+    ok = (res["fitness"] > -1e19) & np.isfinite(adj) & np.isfinite(tan)
+    assert ok.mean() > 0.95
+    rel = np.abs(adj - tan)[ok] / np.maximum(np.abs(tan[ok]), 1e-30)
+    assert np.median(rel) < 2e-4, np.median(rel)
+    assert (rel < 1e-3).mean() >= 0.9, (rel < 1e-3).mean()
+    assert (rel < 1e-2).mean() >= 0.97, (rel < 1e-2).mean()
+
+
+def test_tangent_refuses_other_worlds(engine):
+    world = WORKLOADS["refine"].world(duration=0.5)
+    wave = ce.pack(ce.generate(WORKLOADS["refine"].spec, 16), world)
+    with engine.forward(wave, world) as tape:
+        rows, _ = tape.shape
+        with pytest.raises(ce.EngineError) as err:
+            tape.tangent(np.zeros((len(wave), rows, 2), np.float32))
+    assert err.value.status == ce.CE_ERR_UNSUPPORTED
