@@ -1172,14 +1172,14 @@ size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block) {
 bool tangent_world(uint32_t flags) { return flags == kWorldCalm; }
 
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
-                           float* dfitness) {
+                           const float* dmuscle, const float* dfriction, float* dfitness) {
     if (s.record || a.rows != s.rows || a.mm != s.mm || !tangent_world(s.flags)) return cudaErrorInvalidValue;
     const size_t smem = tangent_smem_bytes(s.rows, s.mm, s.block);
     auto at = [&](auto r) -> cudaError_t {
         auto kern = tangent_kernel<CalmWorld, decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, dstart, dfitness);
+        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, dstart, dmuscle, dfriction, dfitness);
         return cudaGetLastError();
     };
     if (s.rate == 60) return at(std::integral_constant<int, 60>{});

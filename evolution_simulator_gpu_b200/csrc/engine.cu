@@ -952,19 +952,15 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
     return CE_OK;
 }
 
-extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, size_t cap_floats, float* dfitness) {
-    if (!t || !dstart || !dfitness) {
-        set_error("ce_tangent: null argument");
+extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dmuscle, const float* dfriction,
+                                float* dfitness) {
+    if (!t || !dfitness || (!dstart && !dmuscle && !dfriction)) {
+        set_error("ce_tangent: null argument (a tape, the output and at least one direction)");
         return CE_ERR_INVALID;
     }
     if (!cek::tangent_world(t->flags)) {
         set_error("ce_tangent: the tangent-linear run is built for the calm world");
         return CE_ERR_UNSUPPORTED;
-    }
-    const size_t per = 2u * (size_t)t->rows;
-    if (cap_floats < t->count * per) {
-        set_error("ce_tangent: direction buffer too small, need " + std::to_string(t->count * per) + " floats");
-        return CE_ERR_INVALID;
     }
     if (cek::tangent_smem_bytes(t->rows, t->mm, cek::kBlock) > t->engine->smem_optin) {
         set_error("ce_tangent: bodies too large for the tangent run's shared memory");
@@ -972,31 +968,48 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, size_t cap_floa
     }
     ce_status s = set_device(t->engine);
     if (s != CE_OK) return s;
-    const size_t needed = (t->count + cek::kBlock - 1) / cek::kBlock;
+    const size_t n = t->count;
+    const size_t start_b = n * 2u * t->rows * 4u, muscle_b = n * (size_t)cek::kGradMuscle * t->mm * 4u,
+                 friction_b = n * (size_t)t->rows * 4u;
+    const size_t needed = (n + cek::kBlock - 1) / cek::kBlock;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min(needed, (size_t)t->engine->sms));
-    // The direction and the result live only for this call.
+    // The directions and the result live only for this call.
     struct Owned {
         DeviceBuf buf;
         ~Owned() { buf.release(); }
     } dir, out;
-    DeviceBuf& d_dir = dir.buf;
-    DeviceBuf& d_out = out.buf;
-    if ((s = t->d_scratch.ensure(cek::adjoint_slot_bytes(grid, t->rows, t->mm))) ||
-        (s = d_dir.ensure(t->count * per * 4)) || (s = d_out.ensure(t->count * 4))) {
+    const size_t dir_b = (dstart ? start_b : 0) + (dmuscle ? muscle_b : 0) + (dfriction ? friction_b : 0);
+    if ((s = t->d_scratch.ensure(cek::adjoint_slot_bytes(grid, t->rows, t->mm))) || (s = dir.buf.ensure(dir_b)) ||
+        (s = out.buf.ensure(n * 4))) {
         return s;
     }
     cudaStream_t st = t->stream;
-    CE_TRY(cudaMemcpyAsync(d_dir.ptr, dstart, t->count * per * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-    CE_TRY(cudaMemsetAsync(d_out.ptr, 0, t->count * 4, st), "cudaMemsetAsync");
-    const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, t->count);
-    CE_TRY(cek::launch_bucket(static_cast<const uint4*>(t->d_heads.ptr), 0u, (uint32_t)t->count, bk, st),
+    char* at = static_cast<char*>(dir.buf.ptr);
+    const float *d_start = nullptr, *d_muscle = nullptr, *d_friction = nullptr;
+    if (dstart) {
+        CE_TRY(cudaMemcpyAsync(at, dstart, start_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        d_start = reinterpret_cast<const float*>(at);
+        at += start_b;
+    }
+    if (dmuscle) {
+        CE_TRY(cudaMemcpyAsync(at, dmuscle, muscle_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        d_muscle = reinterpret_cast<const float*>(at);
+        at += muscle_b;
+    }
+    if (dfriction) {
+        CE_TRY(cudaMemcpyAsync(at, dfriction, friction_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        d_friction = reinterpret_cast<const float*>(at);
+    }
+    CE_TRY(cudaMemsetAsync(out.buf.ptr, 0, n * 4, st), "cudaMemsetAsync");
+    const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, n);
+    CE_TRY(cek::launch_bucket(static_cast<const uint4*>(t->d_heads.ptr), 0u, (uint32_t)n, bk, st),
            "bucketing launch");
     cek::KernelArgs a = tape_args(t, bk);
     a.scratch = static_cast<float4*>(t->d_scratch.ptr);
     cek::LaunchSpec ls{t->rows, t->mm, t->flags, false, t->rate, grid, cek::kBlock, st};
-    CE_TRY(cek::launch_tangent(ls, a, t->params, static_cast<const float*>(d_dir.ptr), static_cast<float*>(d_out.ptr)),
+    CE_TRY(cek::launch_tangent(ls, a, t->params, d_start, d_muscle, d_friction, static_cast<float*>(out.buf.ptr)),
            "tangent launch");
-    CE_TRY(cudaMemcpyAsync(dfitness, d_out.ptr, t->count * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    CE_TRY(cudaMemcpyAsync(dfitness, out.buf.ptr, n * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     CE_TRY(cudaStreamSynchronize(st), "tangent run");
     return CE_OK;
 }

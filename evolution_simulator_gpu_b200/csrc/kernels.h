@@ -97,13 +97,15 @@ cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, uint32_t flags, int ra
 struct LaunchSpec;
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
 // The tangent-linear run (the adjoint's check; calm world only): d fitness
-// of each creature along start-position tangents dstart (2 x rows floats a
-// creature, packed index) into dfitness, on the lane slots of
-// adjoint_slot_bytes and the checkpointed forward run's ends and results.
+// of each creature along directions of its start positions (dstart, 2 x
+// rows floats a creature), muscle record fields (dmuscle, kGradMuscle x mm)
+// and node frictions (dfriction, rows), packed index, each null for 0, into
+// dfitness, on the lane slots of adjoint_slot_bytes and the checkpointed
+// forward run's ends and results.
 size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block);
 bool tangent_world(uint32_t flags);
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
-                           float* dfitness);
+                           const float* dmuscle, const float* dfriction, float* dfitness);
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
                            const float* weights);
 

@@ -1,7 +1,8 @@
 // The tangent-linear run of a creature's trial (included by adjoint.cu,
 // inside its namespace, after Backward): the forward derivative of the
-// fitness along a direction of the start positions, carried substep by
-// substep beside the FP32 trajectory itself.
+// fitness along a direction of the start positions, the muscles' record
+// fields and the nodes' friction, carried substep by substep beside the
+// FP32 trajectory itself.
 //
 // Each substep first takes the derivative of the muscle pass from the
 // substep's start state, then runs the forward substep through
@@ -9,8 +10,8 @@
 // joint-limit mode are those of the creature kernel, to the bit), then the
 // derivative of each later pass in the forward order from the values that
 // pass saw (the kept lines). Every pass here is the transpose of the
-// backward run's reverse pass, so for a direction u of the start positions
-// <adjoint gradient, u> equals the tangent's d fitness up to the rounding of
+// backward run's reverse pass, so for a direction u <adjoint gradient, u>
+// equals the tangent's d fitness up to the rounding of
 // the two FP32 derivative computations: a check of the adjoint that does not
 // depend on a second trajectory (an FP64 tangent takes its own contact
 // modes). Worlds without water, wind, mud or brambles (the world forces are
@@ -21,10 +22,45 @@ struct Tangent {
     using Body = typename B::Body;
     using C = Clock<RATE>;
     const B& bw;
-    const NodeTables& d;  // tangents: positions, velocities, muscle forces then start positions, (energy, -)
+    const NodeTables& d;  // tangents: positions, velocities, muscle forces then start positions, (energy, demand)
+    // The creature's parameter directions: 9 floats a muscle slot in the
+    // gradient's order (amplitude, hill, cap, 1/capacity, phase, duty,
+    // 1/duty, 1/(1-duty), stiffness), one friction a node row; null for 0.
+    const float* du_muscle;
+    const float* du_friction;
 
-    // d (a, b) with a and b 2-vectors.
-    __device__ __forceinline__ static float dot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+    __device__ __forceinline__ float mu_dir(unsigned k, unsigned f) const {
+        return du_muscle ? du_muscle[kGradMuscle * k + f] : 0.0f;
+    }
+
+    // Tangent of the step's demands (Creature::muscle_demands; the
+    // transpose of Backward::demands_back) into d.muscle().y.
+    __device__ __forceinline__ void demands_tan(float t_now) const {
+        const Body& b = bw.b;
+        const LaneRegs& r = b.r;
+        const Lines& L = b.L;
+        const SlotLayout& S = b.S;
+        for (unsigned k = 0u; k < r.muscles; k++) {
+            const unsigned m0 = S.muscle + 5u * k;
+            const float4 r0 = L.get_cold(m0 + kRhythm0), r1 = L.get_cold(m0 + kRhythm1);
+            const float offset = L.word_cold(m0 + kMState, 2);
+            const float before = rhythm(t_now, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
+            const float after = rhythm(t_now + C::dt, r0.y, r0.z, offset, r0.w, r1.x, r1.y);
+            const float shortening = r0.x * (after - before) * C::rate;
+            const float xd = shortening * r1.z * 0.25f;
+            float dd = 0.0f;
+            if (!r.limp && xd >= 0.0f && du_muscle) {
+                float4 ga = make_float4(0.0f, 0.0f, 0.0f, 0.0f), gb = ga;
+                B::rhythm_back(t_now + C::dt, r0, r1, offset, 1.0f, ga);
+                B::rhythm_back(t_now, r0, r1, offset, 1.0f, gb);
+                const float da = ga.x * mu_dir(k, 4) + ga.y * mu_dir(k, 5) + ga.z * mu_dir(k, 6) + ga.w * mu_dir(k, 7);
+                const float db = gb.x * mu_dir(k, 4) + gb.y * mu_dir(k, 5) + gb.z * mu_dir(k, 6) + gb.w * mu_dir(k, 7);
+                const float dshort = (mu_dir(k, 0) * (after - before) + r0.x * (da - db)) * C::rate;
+                dd = (dshort * r1.z + shortening * mu_dir(k, 8)) * 0.25f;
+            }
+            d.muscle(k).y = dd;
+        }
+    }
 
     // Tangent of the muscle pass (Creature::muscle_forces) from the start
     // state in the tables: the muscle forces' tangents into d.f and the new
@@ -71,23 +107,25 @@ struct Tangent {
             const float drvx = dvb.x - dva.x, drvy = dvb.y - dva.y;
             const float lengthening = rvx * ex + rvy * ey;
             const float dlg = drvx * ex + rvx * dex + drvy * ey + rvy * dey;
-            // The demand depends on time and the muscle's genes only.
-            const float drive0 = ms.y * ms.x, ddrive0 = ms.y * d.muscle(k).x;
+            const float dhill = mu_dir(k, 1), dcap = mu_dir(k, 2), dicap = mu_dir(k, 3);
+            const float drive0 = ms.y * ms.x, ddrive0 = ms.y * d.muscle(k).x + d.muscle(k).y * ms.x;
             float drive = drive0, ddrive = ddrive0;
             if (hill > 0.0f) {
                 const float hz = 1.0f + lengthening * hill;
                 const float hc = clampf(hz, 0.0f, 1.0f);
                 drive = drive0 * hc;
-                ddrive = ddrive0 * hc + ((hz >= 0.0f && hz <= 1.0f) ? drive0 * dlg * hill : 0.0f);
+                ddrive = ddrive0 * hc +
+                         ((hz >= 0.0f && hz <= 1.0f) ? drive0 * (dlg * hill + lengthening * dhill) : 0.0f);
             }
             const float ya = drive + lengthening * 0.15f;
-            const float dactive = (ya >= -cap && ya <= cap) ? ddrive + 0.15f * dlg : 0.0f;
+            const float dactive = (ya >= -cap && ya <= cap) ? ddrive + 0.15f * dlg : (ya > cap ? dcap : -dcap);
             const float active = clampf(ya, -cap, cap);
             const float m1 = fminf(drive, cap), m2 = fmaxf(-lengthening, 0.0f);
-            const float dm1 = drive <= cap ? ddrive : 0.0f, dm2 = -lengthening >= 0.0f ? -dlg : 0.0f;
+            const float dm1 = drive <= cap ? ddrive : dcap, dm2 = -lengthening >= 0.0f ? -dlg : 0.0f;
             const float work = m1 * m2 * C::h, dwork = (dm1 * m2 + m1 * dm2) * C::h;
             const float z = ms.x - work * inv_capacity * p.inv_muscle_energy + c * (1.0f - ms.x);
-            const float dz = d.muscle(k).x * (1.0f - c) - dwork * inv_capacity * p.inv_muscle_energy;
+            const float dz = d.muscle(k).x * (1.0f - c) -
+                             (dwork * inv_capacity + work * dicap) * p.inv_muscle_energy;
             d.muscle(k).x = (z >= 0.0f && z <= 1.0f) ? dz : 0.0f;
             const float pull = active + tendon_k * fmaxf(len - slack, 0.0f);
             const float dpull = dactive + (len - slack >= 0.0f ? tendon_k * dlen : 0.0f);
@@ -294,9 +332,9 @@ struct Tangent {
             const float dsec = Sl * dS / sec;
             const float dnx = -dS / sec + Sl * dsec / (sec * sec), dny = -dsec / (sec * sec);
             const float ddepth = -((dq.y - dh) / sec - (q.y - c.gr.x) * dsec / (sec * sec));
-            float dmu = 0.0f;
+            float dmu = du_friction ? du_friction[i] * p.friction * c.ice : 0.0f;
             if (b.w.has(CE_FLAG_ICE)) {
-                dmu = -nr.w * p.friction * p.patches * ice_slope(q.x) * dq.x;
+                dmu -= nr.w * p.friction * p.patches * ice_slope(q.x) * dq.x;
             }
             const float2 dq1 = make_float2(dq.x + dnx * c.depth + c.n.x * ddepth, dq.y + dny * c.depth + c.n.y * ddepth);
             const float tx = c.n.y, ty = -c.n.x, dtx = dny, dty = -dnx;
@@ -361,8 +399,9 @@ struct Tangent {
     }
 
     // Runs creature `cidx`'s trial with the tangent of its start positions
-    // `dstart` (2 x rows floats, (x, y) per node row) and returns d fitness;
-    // 0 for a trial that failed or ran no step.
+    // `dstart` (2 x rows floats, (x, y) per node row, null for 0) and of the
+    // parameters (du_muscle, du_friction) and returns d fitness; 0 for a
+    // trial that failed or ran no step.
     __device__ __forceinline__ float run(unsigned cidx, const float* dstart) const {
         const Body& b = bw.b;
         const KernelArgs& a = bw.a;
@@ -373,7 +412,7 @@ struct Tangent {
             return 0.0f;
         }
         for (unsigned i = 0u; i < r.nodes; i++) {
-            d.pos(i) = make_float2(dstart[2u * i], dstart[2u * i + 1u]);
+            d.pos(i) = dstart ? make_float2(dstart[2u * i], dstart[2u * i + 1u]) : make_float2(0.0f, 0.0f);
             d.vel(i) = make_float2(0.0f, 0.0f);
         }
         for (unsigned k = 0u; k < r.muscles; k++) {
@@ -381,6 +420,7 @@ struct Tangent {
         }
         for (unsigned s = 0u; s < end; s++) {
             b.muscle_demands((float)s * C::dt);
+            demands_tan((float)s * C::dt);
             for (unsigned q = 0u; q < 16u; q++) {
                 muscles_tan();
                 unsigned touch, slip;
@@ -404,6 +444,7 @@ struct Tangent {
 
 template <class W, int RATE>
 __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, const ce_params p, const float* dstart,
+                                                            const float* dmuscle, const float* dfriction,
                                                             float* dfitness) {
     extern __shared__ float4 smem[];
     using B = Backward<W, RATE>;
@@ -431,7 +472,6 @@ __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, 
     unsigned end = 0u, seg = 0u;
     float weight = 1.0f;
     const B back{body, tan, nullptr, A, tape, a, x, end, seg, weight};
-    const Tangent<W, RATE> tl{back, tan};
     const size_t per = 2u * (size_t)a.rows;
     Claim claim(a, lane, warp, warps_total);
     for (;;) {
@@ -444,7 +484,9 @@ __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, 
         }
         if (mine != kNone) {
             const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
-            dfitness[cidx] = tl.run(cidx, dstart + (size_t)cidx * per);
+            const Tangent<W, RATE> tl{back, tan, dmuscle ? dmuscle + (size_t)cidx * kGradMuscle * a.mm : nullptr,
+                                      dfriction ? dfriction + (size_t)cidx * a.rows : nullptr};
+            dfitness[cidx] = tl.run(cidx, dstart ? dstart + (size_t)cidx * per : nullptr);
         }
     }
 }
