@@ -231,6 +231,23 @@ def ascend(pop: api.Population, muscle_grads: np.ndarray, node_grads: np.ndarray
     return out
 
 
+def pick(cands, choice: np.ndarray, fallback: api.Population) -> api.Population:
+    """Per creature c the genes of cands[choice[c]] (-1: `fallback`'s). The
+    candidates and the fallback share one layout (ascend keeps it)."""
+    out = api.Population(fallback.nodes.copy(), fallback.bones.copy(), fallback.muscles.copy(),
+                         fallback.genomes.copy(), None if fallback.strength is None else fallback.strength.copy())
+    m_own = _owner(out, "muscle_start", "muscle_count")
+    n_own = _owner(out, "node_start", "node_count")
+    for j, cand in enumerate(cands):
+        mrows = choice[m_own] == j
+        out.muscles[mrows] = cand.muscles[mrows]
+        if out.strength is not None:
+            out.strength[mrows] = cand.strength[mrows]
+        nrows = choice[n_own] == j
+        out.nodes[nrows] = cand.nodes[nrows]
+    return out
+
+
 def _fitness(wave: api.WavePack, results: np.ndarray) -> np.ndarray:
     """Fitness in population order from results in packed order."""
     out = np.empty(len(wave), np.float32)
@@ -254,7 +271,7 @@ def _evaluate(engine, pop, world, chunk: int):
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
            resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None,
-           sampler: str = "host", guided: bool = False, ascent: str = "device") -> dict:
+           sampler: str = "host", guided: bool = False, ascent: str = "device", line_search=()) -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -280,7 +297,12 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     `ascent` "device" runs the ascent steps and the last scoring as one CUDA
     graph on the GPU (api.Ascent: no host round trip between the steps),
     "host" step by step through the host (packing, gene gradients and the
-    step in numpy); both give the same fitness and genes."""
+    step in numpy); both give the same fitness and genes. With
+    `line_search` (step-size factors, e.g. (0.25, 1, 4, 16)), a further arm
+    runs `steps` ascent steps whose size each creature chooses: per step one
+    gradient (checkpointed forward and backward run), then one evaluation of
+    each factor's step, and each creature moves to its best candidate if
+    that beats where it stands; its GPU time counts every evaluation."""
     draw = samples if sampler == "host" else samples_gpu
     report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
                   ranks=world_size, sampler=sampler, ascent=ascent)
@@ -378,6 +400,37 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         report["resample"] = dict(children_per_elite=tr[3] / world_size, gpu_s=tr[2], mean_best=tr[0] / n_el,
                                   gain=gain_r, gain_per_gpu_s=gain_r / tr[2], improved=tr[1] / n_el,
                                   host_s=time.perf_counter() - t0)
+    if line_search and len(mine):
+        t0 = time.perf_counter()
+        xl, fl = elite, f0.astype(np.float64)
+        bestl, secs = f0.copy(), 0.0
+        for k in range(steps):
+            wave = api.pack(xl, world)
+            with engine.forward(wave, world) as tape:
+                g = tape.backward()
+                shape = tape.shape
+                fwd, bwd = tape.seconds
+            secs += fwd + bwd
+            mg, ng = api.gene_gradients(xl, wave, world, g, shape)
+            cands, fits = [], []
+            for f in line_search:
+                cand = ascend(xl, mg, ng, step * f)
+                fc, busy_c = _evaluate(engine, cand, world, chunk)
+                secs += busy_c
+                cands.append(cand)
+                fits.append(np.where(fc > -1e19, fc, -np.inf).astype(np.float64))
+            fits = np.stack(fits)
+            j = np.argmax(fits, axis=0)
+            better = fits[j, np.arange(len(j))] > fl
+            choice = np.where(better, j, -1)
+            xl = pick(cands, choice, xl)
+            fl = np.where(better, fits[j, np.arange(len(j))], fl)
+            bestl = np.maximum(bestl, fl)
+        tl = shard.all_sum([bestl.sum(), (bestl > f0).sum(), secs], world_size, group, device)
+        gain_l = (tl[0] - tot[1]) / n_el
+        report["line"] = dict(factors=list(line_search), gpu_s=tl[2], mean_best=tl[0] / n_el, gain=gain_l,
+                              gain_per_gpu_s=gain_l / max(tl[2], 1e-12), improved=tl[1] / n_el,
+                              host_s=time.perf_counter() - t0)
     if guided:
         t0 = time.perf_counter()
         if stepped is None:

@@ -97,6 +97,24 @@ def test_ascent_step_follows_the_gradient_within_its_clip():
     assert _same(bad.nodes, pop.nodes)
 
 
+def test_pick_takes_each_creatures_genes_from_its_chosen_candidate():
+    pop = ce.generate(W.spec, 24)
+    pop.strength = np.ones(len(pop.muscles), np.float32)
+    rng = np.random.default_rng(4)
+    cands = [refine.ascend(pop, rng.normal(size=(len(pop.muscles), 5)), rng.normal(size=len(pop.nodes)), 1e-2)
+             for _ in range(3)]
+    choice = rng.integers(-1, 3, size=len(pop))
+    out = refine.pick(cands, choice, pop)
+    for c in range(len(pop)):
+        src = pop if choice[c] < 0 else cands[choice[c]]
+        want, got = src.creature(c), out.creature(c)
+        for a, b in zip(want[:3], got[:3]):
+            assert _same(a, b), c
+        g = pop.genomes[c]
+        sl = slice(int(g["muscle_start"]), int(g["muscle_start"] + g["muscle_count"]))
+        assert _same(out.strength[sl], src.strength[sl]), c
+
+
 def test_host_samples_do_not_depend_on_the_range():
     """A sample's moves come from its block's own stream: drawing samples
     [0, 10000) at once or as [0, 3000) and [3000, 10000) gives the same
