@@ -507,10 +507,20 @@ struct Backward {
         const ce_params& p = b.p;
         const unsigned bones = r.nodes - 1u;
         // Damping, joints from last to first; positions are those after the
-        // ground pass (the table holds them).
+        // ground pass (the table holds them). Here and in the bone, node,
+        // drag and muscle loops below, the next item's lines load while the
+        // current item is worked on; the extra load at a loop's end reads an
+        // item of the creature's own (joint 0, bone 0) or the line after the
+        // last, which the slot holds.
         const float share = fminf(C::h * kInvJointDamping, 1.0f);
+        float4 na = L.get(S.joint + 2u * (bones - 1u)), nb = L.get(S.joint + 2u * (bones - 1u) + 1u);
+        float4 nd0 = L.get(A.damp + 2u * (bones - 1u)), nd1 = L.get(A.damp + 2u * (bones - 1u) + 1u);
         for (unsigned j = bones; j-- > 1u;) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = na, rb = nb, d0 = nd0, d1 = nd1;
+            na = L.get(S.joint + 2u * (j - 1u));
+            nb = L.get(S.joint + 2u * (j - 1u) + 1u);
+            nd0 = L.get(A.damp + 2u * (j - 1u));
+            nd1 = L.get(A.damp + 2u * (j - 1u) + 1u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }
@@ -519,7 +529,6 @@ struct Backward {
             if (!(wgt > 0.0f)) {
                 continue;
             }
-            const float4 d0 = L.get(A.damp + 2u * j), d1 = L.get(A.damp + 2u * j + 1u);
             const float2 vt = make_float2(d0.x, d0.y), vf = make_float2(d0.z, d0.w), vh = make_float2(d1.x, d1.y);
             const float rate = k.g_tip.x * vt.x + k.g_tip.y * vt.y + k.g_far.x * vf.x + k.g_far.y * vf.y +
                                k.g_hub.x * vh.x + k.g_hub.y * vh.y;
@@ -579,9 +588,12 @@ struct Backward {
             joint_limit_back(j, ra, rb, e0, e1);
         }
         // Bone lengths, last to first.
+        float4 nba = L.get(S.bone + 2u * (bones - 1u)), npre = L.get(A.bones + bones - 1u);
         for (unsigned j = bones; j-- > 0u;) {
-            const float4 ba = L.get(S.bone + 2u * j);
-            const float4 pre = L.get(A.bones + j);
+            const float4 ba = nba, pre = npre;
+            const unsigned jn = j > 0u ? j - 1u : 0u;
+            nba = L.get(S.bone + 2u * jn);
+            npre = L.get(A.bones + jn);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float dx = pre.z - pre.x, dy = pre.w - pre.y;
             const float len0 = sqrtf(dx * dx + dy * dy);
@@ -608,8 +620,13 @@ struct Backward {
         // kept for the velocity pass. Mass: the world force is a mass times
         // an acceleration (gravity, wind, buoyancy), so the m-derivative of
         // v1 is -a h F / m^2. Buoyancy's depth goes to the start height.
+        float4 nnr = L.get(S.node);
+        float2 nF = reinterpret_cast<const float2*>(&L.base[A.force * 32u])[0];
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
+            const float4 nr = nnr;
+            const float2 F = nF;
+            nnr = L.get(S.node + i + 1u);
+            nF = reinterpret_cast<const float2*>(&L.base[(A.force + (i + 1u) / 2u) * 32u])[(i + 1u) % 2u];
             const float im = nr.y;
             const float2 lq1 = g.pos(i), lq0 = g.f(i);
             float2 lp = make_float2(lq1.x + lq0.x, lq1.y + lq0.y);
@@ -628,13 +645,17 @@ struct Backward {
             g.pos(i) = lp;
             g.vel(i) = lv1;
             g.f(i) = make_float2(lv1.x * C::h * im, lv1.y * C::h * im);
-            const float2 F = reinterpret_cast<const float2*>(&L.base[(A.force + i / 2u) * 32u])[i % 2u];
             add_mass(i, -C::h * im * im * (lv1.x * F.x + lv1.y * F.y));
         }
         // Bone drag, last to first.
+        float4 dba = L.get(S.bone + 2u * (bones - 1u)), dbb = L.get(S.bone + 2u * (bones - 1u) + 1u);
+        float4 dpre = L.get(A.drag + bones - 1u);
         for (unsigned j = bones; j-- > 0u;) {
-            const float4 ba = L.get(S.bone + 2u * j), bb = L.get(S.bone + 2u * j + 1u);
-            const float4 pre = L.get(A.drag + j);
+            const float4 ba = dba, bb = dbb, pre = dpre;
+            const unsigned jn = j > 0u ? j - 1u : 0u;
+            dba = L.get(S.bone + 2u * jn);
+            dbb = L.get(S.bone + 2u * jn + 1u);
+            dpre = L.get(A.drag + jn);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float wx = 0.5f * (pre.x + pre.z), wy = 0.5f * (pre.y + pre.w);
             const float speed = sqrtf(wx * wx + wy * wy);
@@ -829,11 +850,17 @@ struct Backward {
         const SlotLayout& S = b.S;
         const ce_params& p = b.p;
         const float c = kMuscleRecovery * p.muscle_recovery * C::h;
+        float4 n0 = L.get(S.muscle + kPull0), nacc = L.get(A.grad);
+        float2 nc = L.get2(S.cap, 0u), nt = r.tendon ? L.get2(S.tendon, 0u) : make_float2(0.0f, 0.0f);
         for (unsigned k = 0u; k < r.muscles; k++) {
-            const unsigned m0 = S.muscle + 5u * k;
-            const float4 q0 = L.get(m0 + kPull0);
-            const float2 qc = L.get2(S.cap, k);
-            const float2 qt = r.tendon ? L.get2(S.tendon, k) : make_float2(0.0f, 0.0f);
+            const float4 q0 = n0, acc = nacc;
+            const float2 qc = nc, qt = nt;
+            n0 = L.get(S.muscle + 5u * (k + 1u) + kPull0);
+            nacc = L.get(A.grad + 3u * (k + 1u));
+            nc = L.get2(S.cap, k + 1u);
+            if (r.tendon) {
+                nt = L.get2(S.tendon, k + 1u);
+            }
             const float4 q1 = make_float4(qc.x, qc.y, qt.x, qt.y);
             const float2 ms = t.muscle(k);
             const unsigned nodes = __float_as_uint(q0.x);
@@ -947,7 +974,7 @@ struct Backward {
             e = g.vel(b1);
             g.vel(b1) = make_float2(e.x + anchor_b * lrvx, e.y + anchor_b * lrvy);
             g.muscle(k) = make_float2(le, lm.y + ld);
-            add_line(A.grad + 3u * k, make_float4(0.0f, g_hill, g_cap, g_icap));
+            L.put(A.grad + 3u * k, make_float4(acc.x + 0.0f, acc.y + g_hill, acc.z + g_cap, acc.w + g_icap));
         }
     }
 
