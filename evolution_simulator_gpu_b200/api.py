@@ -217,6 +217,7 @@ def _bind(lib: C.CDLL) -> None:
         "ce_tape_shape": (C.c_int, [C.c_void_p, P(C.c_uint32), P(C.c_uint32)]),
         "ce_tape_seconds": (C.c_int, [C.c_void_p, P(C.c_double), P(C.c_double)]),
         "ce_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+        "ce_backward_checked": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
         "ce_tape_free": (C.c_int, [C.c_void_p]),
         "ce_tangent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_tape_checkpoints": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(C.c_uint32)]),
@@ -247,7 +248,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_ascent_fitness", "ce_ascent_genes", "ce_ascent_close", "ce_inject_fault", "ce_measure_fp32",
             "ce_to_metrics_batch", "ce_niche_batch", "ce_ground", "ce_quake_hash", "ce_advance_device_noalloc",
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
-            "ce_tape_seconds", "ce_backward", "ce_tape_free", "ce_tangent", "ce_gene_gradients", "ce_tape_checkpoints",
+            "ce_tape_seconds", "ce_backward", "ce_backward_checked", "ce_tape_free", "ce_tangent", "ce_gene_gradients", "ce_tape_checkpoints",
             "ce_replay_decode", "ce_sample_rows", "ce_sample_device", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
             "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
 
@@ -824,16 +825,23 @@ class Tape:
         _check(lib().ce_tape_seconds(self._handle(), C.byref(f), C.byref(b)), "ce_tape_seconds")
         return f.value, b.value
 
-    def backward(self, dl_dfitness=None) -> np.ndarray:
+    def backward(self, dl_dfitness=None, check: bool = False):
         """d(sum_c dl_dfitness[c] fitness_c) / d(record fields), one row per
         creature in packed order: 9 floats a muscle slot (GRAD_MUSCLE_FIELDS),
         then per node row its friction, then its mass, then its start
-        position as (x, y) pairs."""
+        position as (x, y) pairs. With `check`, (gradients, mismatches):
+        ce_backward_checked's per-creature bits of reruns that did not
+        reproduce the forward run (0: none)."""
         per = int(lib().ce_tape_grad_floats(self._handle()))
         out = np.zeros((self.count, per), np.float32)
         w = None if dl_dfitness is None else np.ascontiguousarray(dl_dfitness, np.float32)
         if w is not None and len(w) != self.count:
             raise ValueError("one weight a creature")
+        if check:
+            bad = np.zeros(self.count, np.uint32)
+            _check(lib().ce_backward_checked(self._handle(), _ptr(w), _ptr(out), out.size, _ptr(bad)),
+                   "ce_backward_checked")
+            return out, bad
         _check(lib().ce_backward(self._handle(), _ptr(w), _ptr(out), out.size), "ce_backward")
         return out
 

@@ -124,6 +124,11 @@ struct AdjointArgs {
     float4* tape;           // segment tapes: warps of the grid x 256 substeps x tape lines x 32 lanes
     float* grads;           // grad_floats(rows, mm) a creature (packed index)
     const float* weights;   // dL/dfitness a creature (packed index), NULL for 1
+    // The reruns' check, NULL for none: per creature (packed index) bit 0
+    // when a segment's rerun from its checkpoint does not end on the next
+    // checkpoint to the bit, bit 1 when a substep's kept rerun does not end
+    // on the next tape state (or checkpoint).
+    uint32_t* mismatch;
 };
 
 template <class W, int RATE>
@@ -240,6 +245,42 @@ struct Backward {
         for (unsigned m = 0u; m < r.muscles; m++) {
             __stcs(tape.word(k, 4u * a.rows + m), b.t.muscle(m).x);
         }
+    }
+
+    // Whether the tables hold tape entry k's state (positions, velocities,
+    // energy stores), to the bit.
+    __device__ __forceinline__ bool same_as_tape(unsigned k) const {
+        const LaneRegs& r = b.r;
+        bool same = true;
+        for (unsigned i = 0u; i < r.nodes; i++) {
+            const float2 q = *tape.pair(k, 2u * i), v = *tape.pair(k, 2u * a.rows + 2u * i);
+            const float2 tq = b.t.pos(i), tv = b.t.vel(i);
+            same = same && __float_as_uint(q.x) == __float_as_uint(tq.x) && __float_as_uint(q.y) == __float_as_uint(tq.y) &&
+                   __float_as_uint(v.x) == __float_as_uint(tv.x) && __float_as_uint(v.y) == __float_as_uint(tv.y);
+        }
+        for (unsigned m = 0u; m < r.muscles; m++) {
+            same = same && __float_as_uint(*tape.word(k, 4u * a.rows + m)) == __float_as_uint(b.t.muscle(m).x);
+        }
+        return same;
+    }
+
+    // Whether the tables hold checkpoint s, to the bit.
+    __device__ __forceinline__ bool same_as_checkpoint(unsigned s) const {
+        const LaneRegs& r = b.r;
+        const size_t n = a.count;
+        const float* c = a.ckpt + (size_t)s * checkpoint_floats(a.rows, a.mm) * n + r.cidx;
+        bool same = true;
+        for (unsigned i = 0u; i < r.nodes; i++) {
+            const float2 tq = b.t.pos(i), tv = b.t.vel(i);
+            same = same && __float_as_uint(c[(2u * i) * n]) == __float_as_uint(tq.x) &&
+                   __float_as_uint(c[(2u * i + 1u) * n]) == __float_as_uint(tq.y) &&
+                   __float_as_uint(c[(2u * a.rows + 2u * i) * n]) == __float_as_uint(tv.x) &&
+                   __float_as_uint(c[(2u * a.rows + 2u * i + 1u) * n]) == __float_as_uint(tv.y);
+        }
+        for (unsigned m = 0u; m < r.muscles; m++) {
+            same = same && __float_as_uint(c[(4u * a.rows + m) * n]) == __float_as_uint(b.t.muscle(m).x);
+        }
+        return same;
     }
 
     __device__ __forceinline__ void load_checkpoint(unsigned s) const {
@@ -1040,6 +1081,9 @@ struct Backward {
                 b.substep();
             }
         }
+        if (x.mismatch && s1 < end && !same_as_checkpoint(s1 / 16u)) {
+            atomicOr(x.mismatch + b.r.cidx, 1u);
+        }
         if (s1 == end) {
             // Fitness com_x = sum m x / sum m: d/dm_i = (x_i - com_x) / sum m.
             const LaneRegs& r = b.r;
@@ -1060,6 +1104,12 @@ struct Backward {
                 load_state(k);
                 unsigned touch, slip;
                 const unsigned violated = substep_kept(touch, slip);
+                if (x.mismatch) {
+                    const bool last = k + 1u == (s1 - s0) * 16u;
+                    if (last ? (s1 < end && !same_as_checkpoint(s1 / 16u)) : !same_as_tape(k + 1u)) {
+                        atomicOr(x.mismatch + b.r.cidx, 2u);
+                    }
+                }
                 reverse_substep(k, violated, touch, slip);
             }
             demands_back(t_now);
@@ -1215,10 +1265,10 @@ cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_pa
 }
 
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
-                           const float* weights) {
+                           const float* weights, uint32_t* mismatch) {
     if (s.record || a.rows != s.rows || a.mm != s.mm) return cudaErrorInvalidValue;
     const size_t smem = adjoint_smem_bytes(s.rows, s.mm, s.block);
-    const AdjointArgs x{tape, grads, weights};
+    const AdjointArgs x{tape, grads, weights, mismatch};
     return with_gradient_world(s.flags, s.rate, [&](auto w, auto r) -> cudaError_t {
         auto kern = adjoint_kernel<decltype(w), decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

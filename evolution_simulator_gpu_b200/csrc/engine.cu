@@ -746,7 +746,7 @@ struct ce_tape {
     int rate = 60;
     ce_params params{};
     DeviceBuf d_lanes, d_muscles, d_heads, d_results, d_buckets, d_ckpt, d_ends, d_scratch, d_tape, d_grads,
-        d_weights;
+        d_weights, d_mismatch;
     std::vector<ce_result> results;
     double forward_seconds = 0.0, backward_seconds = 0.0;
 };
@@ -904,7 +904,11 @@ extern "C" ce_status ce_tape_seconds(ce_tape* t, double* forward, double* backwa
     return CE_OK;
 }
 
-extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* grads, size_t cap_floats) {
+namespace {
+
+// ce_backward and ce_backward_checked: the backward run, with the reruns'
+// check when `mismatches` is not NULL.
+ce_status backward(ce_tape* t, const float* dl_dfitness, float* grads, size_t cap_floats, uint32_t* mismatches) {
     if (!t || !grads) {
         set_error("ce_backward: null argument");
         return CE_ERR_INVALID;
@@ -926,7 +930,8 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
     const size_t slot_b = cek::adjoint_slot_bytes(grid, t->rows, t->mm);
     const size_t grads_b = t->count * per * 4;
     if ((s = t->d_scratch.ensure(slot_b)) || (s = t->d_tape.ensure(cek::adjoint_tape_bytes(grid, t->rows, t->mm))) ||
-        (s = t->d_grads.ensure(grads_b)) || (s = t->d_weights.ensure(t->count * 4))) {
+        (s = t->d_grads.ensure(grads_b)) || (s = t->d_weights.ensure(t->count * 4)) ||
+        (mismatches && (s = t->d_mismatch.ensure(t->count * 4)))) {
         return s;
     }
     cudaStream_t st = t->stream;
@@ -935,6 +940,7 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
                "cudaMemcpyAsync");
     }
     CE_TRY(cudaMemsetAsync(t->d_grads.ptr, 0, grads_b, st), "cudaMemsetAsync");
+    if (mismatches) CE_TRY(cudaMemsetAsync(t->d_mismatch.ptr, 0, t->count * 4, st), "cudaMemsetAsync");
     CE_TRY(cudaEventRecord(t->start, st), "cudaEventRecord");
     const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, t->count);
     CE_TRY(cek::launch_bucket(static_cast<const uint4*>(t->d_heads.ptr), 0u, (uint32_t)t->count, bk, st),
@@ -944,12 +950,31 @@ extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* gr
     cek::LaunchSpec ls{t->rows, t->mm, t->flags, false, t->rate, grid, cek::kBlock, st};
     CE_TRY(cek::launch_adjoint(ls, a, t->params, static_cast<float4*>(t->d_tape.ptr),
                                static_cast<float*>(t->d_grads.ptr),
-                               dl_dfitness ? static_cast<const float*>(t->d_weights.ptr) : nullptr),
+                               dl_dfitness ? static_cast<const float*>(t->d_weights.ptr) : nullptr,
+                               mismatches ? static_cast<uint32_t*>(t->d_mismatch.ptr) : nullptr),
            "backward launch");
     CE_TRY(cudaEventRecord(t->stop, st), "cudaEventRecord");
     if ((s = tape_time(t, &t->backward_seconds)) != CE_OK) return s;
     CE_TRY(cudaMemcpy(grads, t->d_grads.ptr, grads_b, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (mismatches) {
+        CE_TRY(cudaMemcpy(mismatches, t->d_mismatch.ptr, t->count * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    }
     return CE_OK;
+}
+
+}  // namespace
+
+extern "C" ce_status ce_backward(ce_tape* t, const float* dl_dfitness, float* grads, size_t cap_floats) {
+    return backward(t, dl_dfitness, grads, cap_floats, nullptr);
+}
+
+extern "C" ce_status ce_backward_checked(ce_tape* t, const float* dl_dfitness, float* grads, size_t cap_floats,
+                                         uint32_t* mismatches) {
+    if (!mismatches) {
+        set_error("ce_backward_checked: null mismatches");
+        return CE_ERR_INVALID;
+    }
+    return backward(t, dl_dfitness, grads, cap_floats, mismatches);
 }
 
 extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dmuscle, const float* dfriction,
@@ -1019,7 +1044,7 @@ extern "C" ce_status ce_tape_free(ce_tape* t) {
     if (t->engine) cudaSetDevice(t->engine->device);
     if (t->stream) cudaStreamSynchronize(t->stream);
     for (DeviceBuf* b : {&t->d_lanes, &t->d_muscles, &t->d_heads, &t->d_results, &t->d_buckets, &t->d_ckpt,
-                         &t->d_ends, &t->d_scratch, &t->d_tape, &t->d_grads, &t->d_weights}) {
+                         &t->d_ends, &t->d_scratch, &t->d_tape, &t->d_grads, &t->d_weights, &t->d_mismatch}) {
         b->release();
     }
     if (t->start) cudaEventDestroy(t->start);
@@ -1249,7 +1274,7 @@ extern "C" ce_status ce_ascent_open(ce_engine* e, const ce_population* pop, cons
         if (ce == cudaSuccess) ce = cek::launch_bucket(heads_d, 0u, (uint32_t)n, bk, st);
         if (ce == cudaSuccess)
             ce = cek::launch_adjoint(bs, ka, a->params, static_cast<float4*>(a->d_tape.ptr),
-                                     static_cast<float*>(a->d_grads.ptr), nullptr);
+                                     static_cast<float*>(a->d_grads.ptr), nullptr, nullptr);
         if (ce == cudaSuccess)
             ce = cek::launch_gene_grads(dpop, static_cast<const float*>(a->d_trig.ptr),
                                         static_cast<const uint32_t*>(a->d_order.ptr), n, a->world,

@@ -106,8 +106,11 @@ size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block);
 bool tangent_world(uint32_t flags);
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
                            const float* dmuscle, const float* dfriction, float* dfitness);
+// `mismatch` (NULL: no check): per creature, bits of reruns that did not
+// reproduce the forward run to the bit (bit 0 a segment's rerun against the
+// next checkpoint, bit 1 a substep's kept rerun against the next tape state).
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,
-                           const float* weights);
+                           const float* weights, uint32_t* mismatch);
 
 // The device arrays that bucketing writes for `count` creatures, carved from
 // one area of bucket_bytes(count) bytes.

@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, 
     const unsigned warps_total = gridDim.x * (threads >> 5u);
     const Lines L = Lines::make(a.scratch + (size_t)warp * A.lines * 32u, lane);
     const Tape tape{nullptr, 0u};
-    const AdjointArgs x{nullptr, nullptr, nullptr};
+    const AdjointArgs x{nullptr, nullptr, nullptr, nullptr};
     const W w{};
     LaneRegs r;
     const typename B::Body body{w, p, tab, L, S, r};

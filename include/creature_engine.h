@@ -483,6 +483,15 @@ ce_status ce_tape_results(ce_tape* tape, ce_result* out, size_t cap);
 uint32_t ce_tape_grad_floats(ce_tape* tape);
 ce_status ce_tape_seconds(ce_tape* tape, double* forward_seconds, double* backward_seconds);
 ce_status ce_backward(ce_tape* tape, const float* dl_dfitness, float* grads, size_t cap_floats);
+/* ce_backward that also checks its reruns against the forward run, to the
+ * bit: per creature (packed order) `mismatches` gets bit 0 when a
+ * segment's rerun from its checkpoint does not end on the next checkpoint
+ * and bit 1 when a substep's kept rerun does not end on the next tape state;
+ * 0 everywhere means every gradient was taken along the forward run's own
+ * trajectory. Slower than ce_backward (one more read of the state a
+ * substep). */
+ce_status ce_backward_checked(ce_tape* tape, const float* dl_dfitness, float* grads, size_t cap_floats,
+                              uint32_t* mismatches);
 ce_status ce_tape_free(ce_tape* tape);
 /* The tangent-linear run of the tape's batch (calm world): for each
  * creature, the derivative of its fitness along a direction of its record

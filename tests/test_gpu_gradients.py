@@ -339,3 +339,22 @@ def test_tangent_refuses_other_worlds(engine):
         with pytest.raises(ce.EngineError) as err:
             tape.tangent(np.zeros((len(wave), rows, 2), np.float32))
     assert err.value.status == ce.CE_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("name", ["gradients", "refine", "effects"])
+def test_backward_reruns_reproduce_the_forward_run(engine, name):
+    """The backward reruns every segment from its checkpoint and every
+    substep from the segment tape; its gradients are those of the forward
+    run only if those reruns land on the forward run's own states. The
+    checked backward compares, to the bit, each segment's rerun with the
+    next checkpoint and each substep's kept rerun with the next tape state,
+    in the calm world, the refined-search world (tremors) and the effects
+    world, and its gradients equal the unchecked backward's."""
+    w = WORKLOADS[name]
+    world = w.world(duration=2.0)
+    wave = ce.pack(ce.generate(w.spec, 1024), world)
+    with engine.forward(wave, world) as tape:
+        plain = tape.backward()
+        checked, bad = tape.backward(check=True)
+    assert (bad == 0).all(), f"{int((bad != 0).sum())} creatures' reruns left the forward run (bits {np.unique(bad)})"
+    assert (plain.view(np.uint32) == checked.view(np.uint32)).all()
