@@ -298,7 +298,10 @@ struct Backward {
 
     // The substep of Creature::substep, keeping what the reverse passes read.
     // Returns the joints past their range (bit j) and sets `touch` (nodes in
-    // contact) and `slip` (contacts that slid).
+    // contact) and `slip` (contacts that slid). Its passes load the next
+    // item's lines while working on the current one, as the forward passes
+    // do; it must land on the forward run's states to the bit, which the
+    // checked backward (AdjointArgs::mismatch) verifies.
     __device__ __forceinline__ unsigned substep_kept(unsigned& touch, unsigned& slip) const {
         const LaneRegs& r = b.r;
         const NodeTables& t = b.t;
@@ -306,8 +309,11 @@ struct Backward {
         const SlotLayout& S = b.S;
         const unsigned bones = r.nodes - 1u;
         b.muscle_forces();
+        float4 ka = L.get(S.bone), kb = L.get(S.bone + 1u);
         for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = L.get(S.bone + 2u * j), bb = L.get(S.bone + 2u * j + 1u);
+            const float4 ba = ka, bb = kb;
+            ka = L.get(S.bone + 2u * j + 2u);
+            kb = L.get(S.bone + 2u * j + 3u);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float2 v0 = t.vel(i0), v1 = t.vel(i1);
             L.put(A.drag + j, make_float4(v0.x, v0.y, v1.x, v1.y));
@@ -334,8 +340,10 @@ struct Backward {
             t.vel(i0) = make_float2(v0.x + bb.z * dfx, v0.y + bb.z * dfy);
             t.vel(i1) = make_float2(v1.x + bb.w * dfx, v1.y + bb.w * dfy);
         }
+        float4 kn = L.get(S.node);
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
+            const float4 nr = kn;
+            kn = L.get(S.node + i + 1u);
             const float2 f = b.node_force(i, nr);
             float4 s = t.at(i);
             const float2 fpv = t.f(i);
@@ -351,8 +359,10 @@ struct Backward {
             s.y += C::h * s.w;
             t.set_at(i, s);
         }
+        float4 kba = L.get(S.bone);
         for (unsigned j = 0u; j < bones; j++) {
-            const float4 ba = L.get(S.bone + 2u * j);
+            const float4 ba = kba;
+            kba = L.get(S.bone + 2u * j + 2u);
             const unsigned i0 = __float_as_uint(ba.x), i1 = j + 1u;
             const float2 p0 = t.pos(i0), p1 = t.pos(i1);
             L.put(A.bones + j, make_float4(p0.x, p0.y, p1.x, p1.y));
@@ -364,8 +374,11 @@ struct Backward {
             t.pos(i1) = make_float2(p1.x - w1 * sc * dx, p1.y - w1 * sc * dy);
         }
         unsigned violated = 0u;
+        float4 kra = L.get(S.joint + 2u), krb = L.get(S.joint + 3u);
         for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = kra, rb = krb;
+            kra = L.get(S.joint + 2u * j + 2u);
+            krb = L.get(S.joint + 2u * j + 3u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }
@@ -393,8 +406,10 @@ struct Backward {
         }
         touch = 0u;
         slip = 0u;
+        float4 gn = L.get(S.node);
         for (unsigned i = 0u; i < r.nodes; i++) {
-            const float4 nr = L.get(S.node + i);
+            const float4 nr = gn;
+            gn = L.get(S.node + i + 1u);
             float2 q = t.pos(i);
             const float2 f0 = t.f(i);
             float* pj = reinterpret_cast<float*>(&L.base[(A.pj + i / 2u) * 32u]) + 2u * (i % 2u);
@@ -413,8 +428,11 @@ struct Backward {
             }
             t.vel(i) = make_float2((q.x - f0.x) * C::inv_h, (q.y - f0.y) * C::inv_h);
         }
+        float4 dra = L.get(S.joint + 2u), drb = L.get(S.joint + 3u);
         for (unsigned j = 1u; j < bones; j++) {
-            const float4 ra = L.get(S.joint + 2u * j), rb = L.get(S.joint + 2u * j + 1u);
+            const float4 ra = dra, rb = drb;
+            dra = L.get(S.joint + 2u * j + 2u);
+            drb = L.get(S.joint + 2u * j + 3u);
             if (__float_as_uint(ra.x) == kNone) {
                 continue;
             }
@@ -609,15 +627,20 @@ struct Backward {
             g.vel(i) = make_float2(0.0f, 0.0f);
         }
         // Ground contact.
+        // The substep's start positions come from the tape: the forward
+        // force table and the adjoint force table share memory.
+        float4 cn = L.get(S.node);
+        float2 cq = reinterpret_cast<const float2*>(&L.base[A.pj * 32u])[0], cf = *tape.pair(k_tape, 0u);
         for (unsigned i = 0u; i < r.nodes; i++) {
+            const float4 nr = cn;
+            const float2 q = cq, f0 = cf;
+            cn = L.get(S.node + i + 1u);
+            cq = reinterpret_cast<const float2*>(&L.base[(A.pj + (i + 1u) / 2u) * 32u])[(i + 1u) % 2u];
+            cf = *tape.pair(k_tape, 2u * (i + 1u));
             if (((touch >> i) & 1u) == 0u) {
                 continue;
             }
-            const float4 nr = L.get(S.node + i);
-            const float* pj = reinterpret_cast<const float*>(&L.base[(A.pj + i / 2u) * 32u]) + 2u * (i % 2u);
-            // The substep's start position, from the tape: the forward
-            // force table and the adjoint force table share memory.
-            ground_back(i, nr, make_float2(pj[0], pj[1]), *tape.pair(k_tape, 2u * i), ((slip >> i) & 1u) != 0u);
+            ground_back(i, nr, q, f0, ((slip >> i) & 1u) != 0u);
         }
         // Joint limits, last to first, on the joints that were pushed.
         for (unsigned j = bones; j-- > 1u;) {
