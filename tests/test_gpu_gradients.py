@@ -341,18 +341,20 @@ def test_tangent_refuses_other_worlds(engine):
     assert err.value.status == ce.CE_ERR_UNSUPPORTED
 
 
-@pytest.mark.parametrize("name", ["gradients", "refine", "effects"])
-def test_backward_reruns_reproduce_the_forward_run(engine, name):
+@pytest.mark.parametrize("name,count,seconds", [("gradients", 1024, 2.0), ("refine", 1024, 2.0),
+                                                 ("effects", 1024, 2.0), ("gradients", 256, 20.0)])
+def test_backward_reruns_reproduce_the_forward_run(engine, name, count, seconds):
     """The backward reruns every segment from its checkpoint and every
     substep from the segment tape; its gradients are those of the forward
     run only if those reruns land on the forward run's own states. The
     checked backward compares, to the bit, each segment's rerun with the
     next checkpoint and each substep's kept rerun with the next tape state,
     in the calm world, the refined-search world (tremors) and the effects
-    world, and its gradients equal the unchecked backward's."""
+    world, and over config 4's 20 s trials, and its gradients equal the
+    unchecked backward's."""
     w = WORKLOADS[name]
-    world = w.world(duration=2.0)
-    wave = ce.pack(ce.generate(w.spec, 1024), world)
+    world = w.world(duration=seconds)
+    wave = ce.pack(ce.generate(w.spec, count), world)
     with engine.forward(wave, world) as tape:
         plain = tape.backward()
         checked, bad = tape.backward(check=True)
