@@ -847,8 +847,8 @@ class Tape:
 
     def tangent(self, dstart=None, dmuscle=None, dfriction=None) -> np.ndarray:
         """d fitness of each creature along a direction of its record fields
-        by the tangent-linear run on the forward run's FP32 trajectory (calm
-        world): `dstart` [creature, rows, 2] start positions, `dmuscle`
+        by the tangent-linear run on the forward run's FP32 trajectory (the
+        worlds `forward` takes): `dstart` [creature, rows, 2] start positions, `dmuscle`
         [creature, muscle slots, 9] and `dfriction` [creature, rows], packed
         order, laid out as `backward`'s rows (each None for 0). The adjoint's
         check: <backward row, direction> = tangent."""

@@ -1269,22 +1269,19 @@ size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block) {
     return (size_t)block * (rows * 48u + (mm > 0u ? mm : 1u) * 16u);
 }
 
-bool tangent_world(uint32_t flags) { return flags == kWorldCalm; }
+bool tangent_world(uint32_t flags) { return gradient_world(flags); }
 
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
                            const float* dmuscle, const float* dfriction, float* dfitness) {
     if (s.record || a.rows != s.rows || a.mm != s.mm || !tangent_world(s.flags)) return cudaErrorInvalidValue;
     const size_t smem = tangent_smem_bytes(s.rows, s.mm, s.block);
-    auto at = [&](auto r) -> cudaError_t {
-        auto kern = tangent_kernel<CalmWorld, decltype(r)::value>;
+    return with_gradient_world(s.flags, s.rate, [&](auto w, auto r) -> cudaError_t {
+        auto kern = tangent_kernel<decltype(w), decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         kern<<<s.grid, s.block, smem, s.stream>>>(a, p, dstart, dmuscle, dfriction, dfitness);
         return cudaGetLastError();
-    };
-    if (s.rate == 60) return at(std::integral_constant<int, 60>{});
-    if (s.rate == 120) return at(std::integral_constant<int, 120>{});
-    return cudaErrorInvalidValue;
+    });
 }
 
 cudaError_t launch_adjoint(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, float4* tape, float* grads,

@@ -984,7 +984,8 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dm
         return CE_ERR_INVALID;
     }
     if (!cek::tangent_world(t->flags)) {
-        set_error("ce_tangent: the tangent-linear run is built for the calm world");
+        set_error("ce_tangent: the tangent-linear run is built for the gradients' worlds (calm, effects without "
+                  "mud, brambles or gaps)");
         return CE_ERR_UNSUPPORTED;
     }
     if (cek::tangent_smem_bytes(t->rows, t->mm, cek::kBlock) > t->engine->smem_optin) {

@@ -96,7 +96,7 @@ bool gradient_world(uint32_t flags);
 cudaError_t adjoint_occupancy(unsigned rows, unsigned mm, uint32_t flags, int rate, int* blocks);
 struct LaunchSpec;
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
-// The tangent-linear run (the adjoint's check; calm world only): d fitness
+// The tangent-linear run (the adjoint's check; the gradients' worlds): d fitness
 // of each creature along directions of its start positions (dstart, 2 x
 // rows floats a creature), muscle record fields (dmuscle, kGradMuscle x mm)
 // and node frictions (dfriction, rows), packed index, each null for 0, into

@@ -14,8 +14,8 @@
 // equals the tangent's d fitness up to the rounding of
 // the two FP32 derivative computations: a check of the adjoint that does not
 // depend on a second trajectory (an FP64 tangent takes its own contact
-// modes). Worlds without water, wind, mud or brambles (the world forces are
-// then constant).
+// modes). The worlds of the gradients: calm, and the effects worlds with or
+// without tremors (no mud, brambles or gaps).
 template <class W, int RATE>
 struct Tangent {
     using B = Backward<W, RATE>;
@@ -141,12 +141,16 @@ struct Tangent {
         }
     }
 
-    // Tangent of the air drag on the bones (Creature::drag_item), bone by
-    // bone as the pass runs, from the velocities each bone saw (A.drag).
+    // Tangent of the air and water drag on the bones (Creature::drag_item),
+    // bone by bone as the pass runs, from the velocities each bone saw
+    // (A.drag); the water's wet share and the bone's direction come from the
+    // substep's start positions (the forward force table holds them, d.pos
+    // still their tangents: the integration's tangent comes after).
     __device__ __forceinline__ void drag_tan() const {
         const Body& b = bw.b;
         const Lines& L = b.L;
         const SlotLayout& S = b.S;
+        const ce_params& p = b.p;
         const unsigned bones = b.r.nodes - 1u;
         for (unsigned j = 0u; j < bones; j++) {
             const float4 ba = L.get(S.bone + 2u * j), bb = L.get(S.bone + 2u * j + 1u);
@@ -160,24 +164,57 @@ struct Tangent {
             const float dwx = 0.5f * (l0.x + l1.x), dwy = 0.5f * (l0.y + l1.y);
             const float dspeed = speed > 0.0f ? (wx * dwx + wy * dwy) / speed : 0.0f;
             const float dk = bb.x * speed <= limit ? bb.x * dspeed : 0.0f;
-            const float ddfx = -(dwx * k_air + wx * dk), ddfy = -(dwy * k_air + wy * dk);
+            float ddfx = -(dwx * k_air + wx * dk), ddfy = -(dwy * k_air + wy * dk);
+            if (b.w.has(CE_FLAG_WATER)) {
+                const float r0 = L.get(S.node + i0).z, r1 = L.get(S.node + i1).z;
+                const float width = r0 + r1;
+                const float2 p0 = b.t.f(i0), p1 = b.t.f(i1), dp0 = d.pos(i0), dp1 = d.pos(i1);
+                const float z0 = (p.water - (p0.y - r0)) / (2.0f * r0);
+                const float z1 = (p.water - (p1.y - r1)) / (2.0f * r1);
+                const float wet = 0.5f * (clampf(z0, 0.0f, 1.0f) + clampf(z1, 0.0f, 1.0f));
+                const float dwet = 0.5f * ((z0 >= 0.0f && z0 <= 1.0f ? -dp0.y / (2.0f * r0) : 0.0f) +
+                                           (z1 >= 0.0f && z1 <= 1.0f ? -dp1.y / (2.0f * r1) : 0.0f));
+                const float ax = (p1.x - p0.x) / ba.y, ay = (p1.y - p0.y) / ba.y;
+                const float dax = (dp1.x - dp0.x) / ba.y, day = (dp1.y - dp0.y) / ba.y;
+                const float along = wx * ax + wy * ay;
+                const float dalong = dwx * ax + dwy * ay + wx * dax + wy * day;
+                const float lx = ax * along, ly = ay * along;
+                const float dlx = dax * along + ax * dalong, dly = day * along + ay * dalong;
+                const float sx = wx - lx, sy = wy - ly, dsx = dwx - dlx, dsy = dwy - dly;
+                const float xw = kWaterDrag * wet * ba.y * width * speed;
+                const float k_water = fminf(xw, limit);
+                const float dkw = xw <= limit ? kWaterDrag * ba.y * width * (dwet * speed + wet * dspeed) : 0.0f;
+                ddfx -= dsx * k_water + sx * dkw + kWaterAlong * (dlx * k_water + lx * dkw);
+                ddfy -= dsy * k_water + sy * dkw + kWaterAlong * (dly * k_water + ly * dkw);
+            }
             d.vel(i0) = make_float2(l0.x + bb.z * ddfx, l0.y + bb.z * ddfy);
             d.vel(i1) = make_float2(l1.x + bb.w * ddfx, l1.y + bb.w * ddfy);
         }
     }
 
-    // Tangent of the integration (Creature::integrate_item): the world force
-    // is constant here; d.f takes the start positions' tangents.
+    // Tangent of the integration (Creature::integrate_item): of the world
+    // forces (gravity, wind, buoyancy) only the buoyancy moves with the state,
+    // through the wet share of the start height; d.f takes the start
+    // positions' tangents.
     __device__ __forceinline__ void integrate_tan() const {
         const Body& b = bw.b;
         const Lines& L = b.L;
         const SlotLayout& S = b.S;
+        const ce_params& p = b.p;
         for (unsigned i = 0u; i < b.r.nodes; i++) {
-            const float im = L.get(S.node + i).y;
+            const float4 nr = L.get(S.node + i);
+            const float im = nr.y;
             const float2 dp = d.pos(i), dfp = d.f(i);
+            float dfy = 0.0f;
+            if (b.w.has(CE_FLAG_WATER)) {
+                const float z = (p.water - (b.t.f(i).y - nr.z)) / (2.0f * nr.z);
+                if (z >= 0.0f && z <= 1.0f) {
+                    dfy = -kWaterBuoyancy * nr.x * p.gravity * dp.y / (2.0f * nr.z);
+                }
+            }
             float2 dv = d.vel(i);
             dv.x += C::h * dfp.x * im;
-            dv.y += C::h * dfp.y * im;
+            dv.y += C::h * (dfp.y + dfy) * im;
             if (b.w.has(CE_FLAG_AIR)) {
                 dv.x *= b.p.air_sub;
                 dv.y *= b.p.air_sub;

@@ -493,7 +493,7 @@ ce_status ce_backward(ce_tape* tape, const float* dl_dfitness, float* grads, siz
 ce_status ce_backward_checked(ce_tape* tape, const float* dl_dfitness, float* grads, size_t cap_floats,
                               uint32_t* mismatches);
 ce_status ce_tape_free(ce_tape* tape);
-/* The tangent-linear run of the tape's batch (calm world): for each
+/* The tangent-linear run of the tape's batch (the worlds ce_forward takes): for each
  * creature, the derivative of its fitness along a direction of its record
  * fields, on the same FP32 trajectory and contact, slip and joint-limit
  * modes as the forward run. Directions in packed order, laid out as

@@ -331,16 +331,6 @@ def test_adjoint_equals_the_tangent_linear_run(tangent_cases, part, seconds, sha
     assert np.median(diff / np.maximum(np.abs(tan[ok]), 1e-30)) < 2e-4
 
 
-def test_tangent_refuses_other_worlds(engine):
-    world = WORKLOADS["refine"].world(duration=0.5)
-    wave = ce.pack(ce.generate(WORKLOADS["refine"].spec, 16), world)
-    with engine.forward(wave, world) as tape:
-        rows, _ = tape.shape
-        with pytest.raises(ce.EngineError) as err:
-            tape.tangent(np.zeros((len(wave), rows, 2), np.float32))
-    assert err.value.status == ce.CE_ERR_UNSUPPORTED
-
-
 @pytest.mark.parametrize("name,count,seconds", [("gradients", 1024, 2.0), ("refine", 1024, 2.0),
                                                  ("effects", 1024, 2.0), ("gradients", 256, 20.0)])
 def test_backward_reruns_reproduce_the_forward_run(engine, name, count, seconds):
