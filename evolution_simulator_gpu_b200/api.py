@@ -219,7 +219,7 @@ def _bind(lib: C.CDLL) -> None:
         "ce_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
         "ce_backward_checked": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
         "ce_tape_free": (C.c_int, [C.c_void_p]),
-        "ce_tangent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_tangent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ce_tape_checkpoints": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, P(C.c_uint32)]),
         "ce_gene_gradients": (C.c_int, [P(PopulationC), C.c_void_p, C.c_size_t, P(World), C.c_void_p, C.c_void_p,
                                         C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -845,19 +845,20 @@ class Tape:
         _check(lib().ce_backward(self._handle(), _ptr(w), _ptr(out), out.size), "ce_backward")
         return out
 
-    def tangent(self, dstart=None, dmuscle=None, dfriction=None) -> np.ndarray:
+    def tangent(self, dstart=None, dmuscle=None, dfriction=None, dmass=None) -> np.ndarray:
         """d fitness of each creature along a direction of its record fields
         by the tangent-linear run on the forward run's FP32 trajectory (the
         worlds `forward` takes): `dstart` [creature, rows, 2] start positions, `dmuscle`
-        [creature, muscle slots, 9] and `dfriction` [creature, rows], packed
+        [creature, muscle slots, 9], `dfriction` and `dmass` [creature, rows], packed
         order, laid out as `backward`'s rows (each None for 0). The adjoint's
         check: <backward row, direction> = tangent."""
         rows, mm = self.shape
         def arr(x, width):
             return None if x is None else np.ascontiguousarray(x, np.float32).reshape(self.count, width)
         ds, dm, df = arr(dstart, 2 * rows), arr(dmuscle, len(GRAD_MUSCLE_FIELDS) * mm), arr(dfriction, rows)
+        dn = arr(dmass, rows)
         out = np.zeros(self.count, np.float32)
-        _check(lib().ce_tangent(self._handle(), _ptr(ds), _ptr(dm), _ptr(df), _ptr(out)), "ce_tangent")
+        _check(lib().ce_tangent(self._handle(), _ptr(ds), _ptr(dm), _ptr(df), _ptr(dn), _ptr(out)), "ce_tangent")
         return out
 
     def checkpoints(self, steps: int) -> np.ndarray:

@@ -1272,14 +1272,14 @@ size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block) {
 bool tangent_world(uint32_t flags) { return gradient_world(flags); }
 
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
-                           const float* dmuscle, const float* dfriction, float* dfitness) {
+                           const float* dmuscle, const float* dfriction, const float* dmass, float* dfitness) {
     if (s.record || a.rows != s.rows || a.mm != s.mm || !tangent_world(s.flags)) return cudaErrorInvalidValue;
     const size_t smem = tangent_smem_bytes(s.rows, s.mm, s.block);
     return with_gradient_world(s.flags, s.rate, [&](auto w, auto r) -> cudaError_t {
         auto kern = tangent_kernel<decltype(w), decltype(r)::value>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, dstart, dmuscle, dfriction, dfitness);
+        kern<<<s.grid, s.block, smem, s.stream>>>(a, p, dstart, dmuscle, dfriction, dmass, dfitness);
         return cudaGetLastError();
     });
 }

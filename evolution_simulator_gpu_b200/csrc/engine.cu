@@ -978,8 +978,8 @@ extern "C" ce_status ce_backward_checked(ce_tape* t, const float* dl_dfitness, f
 }
 
 extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dmuscle, const float* dfriction,
-                                float* dfitness) {
-    if (!t || !dfitness || (!dstart && !dmuscle && !dfriction)) {
+                                const float* dmass, float* dfitness) {
+    if (!t || !dfitness || (!dstart && !dmuscle && !dfriction && !dmass)) {
         set_error("ce_tangent: null argument (a tape, the output and at least one direction)");
         return CE_ERR_INVALID;
     }
@@ -996,7 +996,7 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dm
     if (s != CE_OK) return s;
     const size_t n = t->count;
     const size_t start_b = n * 2u * t->rows * 4u, muscle_b = n * (size_t)cek::kGradMuscle * t->mm * 4u,
-                 friction_b = n * (size_t)t->rows * 4u;
+                 friction_b = n * (size_t)t->rows * 4u, mass_b = friction_b;
     const size_t needed = (n + cek::kBlock - 1) / cek::kBlock;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min(needed, (size_t)t->engine->sms));
     // The directions and the result live only for this call.
@@ -1004,14 +1004,15 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dm
         DeviceBuf buf;
         ~Owned() { buf.release(); }
     } dir, out;
-    const size_t dir_b = (dstart ? start_b : 0) + (dmuscle ? muscle_b : 0) + (dfriction ? friction_b : 0);
+    const size_t dir_b =
+        (dstart ? start_b : 0) + (dmuscle ? muscle_b : 0) + (dfriction ? friction_b : 0) + (dmass ? mass_b : 0);
     if ((s = t->d_scratch.ensure(cek::adjoint_slot_bytes(grid, t->rows, t->mm))) || (s = dir.buf.ensure(dir_b)) ||
         (s = out.buf.ensure(n * 4))) {
         return s;
     }
     cudaStream_t st = t->stream;
     char* at = static_cast<char*>(dir.buf.ptr);
-    const float *d_start = nullptr, *d_muscle = nullptr, *d_friction = nullptr;
+    const float *d_start = nullptr, *d_muscle = nullptr, *d_friction = nullptr, *d_mass = nullptr;
     if (dstart) {
         CE_TRY(cudaMemcpyAsync(at, dstart, start_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
         d_start = reinterpret_cast<const float*>(at);
@@ -1025,6 +1026,11 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dm
     if (dfriction) {
         CE_TRY(cudaMemcpyAsync(at, dfriction, friction_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
         d_friction = reinterpret_cast<const float*>(at);
+        at += friction_b;
+    }
+    if (dmass) {
+        CE_TRY(cudaMemcpyAsync(at, dmass, mass_b, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        d_mass = reinterpret_cast<const float*>(at);
     }
     CE_TRY(cudaMemsetAsync(out.buf.ptr, 0, n * 4, st), "cudaMemsetAsync");
     const cek::Buckets bk = cek::bucket_layout(t->d_buckets.ptr, n);
@@ -1033,7 +1039,8 @@ extern "C" ce_status ce_tangent(ce_tape* t, const float* dstart, const float* dm
     cek::KernelArgs a = tape_args(t, bk);
     a.scratch = static_cast<float4*>(t->d_scratch.ptr);
     cek::LaunchSpec ls{t->rows, t->mm, t->flags, false, t->rate, grid, cek::kBlock, st};
-    CE_TRY(cek::launch_tangent(ls, a, t->params, d_start, d_muscle, d_friction, static_cast<float*>(out.buf.ptr)),
+    CE_TRY(cek::launch_tangent(ls, a, t->params, d_start, d_muscle, d_friction, d_mass,
+                               static_cast<float*>(out.buf.ptr)),
            "tangent launch");
     CE_TRY(cudaMemcpyAsync(dfitness, out.buf.ptr, n * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
     CE_TRY(cudaStreamSynchronize(st), "tangent run");

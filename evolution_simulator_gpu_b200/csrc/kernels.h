@@ -98,14 +98,15 @@ struct LaunchSpec;
 cudaError_t launch_forward_ckpt(const LaunchSpec& s, const KernelArgs& a, const ce_params& p);
 // The tangent-linear run (the adjoint's check; the gradients' worlds): d fitness
 // of each creature along directions of its start positions (dstart, 2 x
-// rows floats a creature), muscle record fields (dmuscle, kGradMuscle x mm)
-// and node frictions (dfriction, rows), packed index, each null for 0, into
+// rows floats a creature), muscle record fields (dmuscle, kGradMuscle x mm),
+// node frictions (dfriction, rows) and node masses (dmass, rows), packed
+// index, each null for 0, into
 // dfitness, on the lane slots of adjoint_slot_bytes and the checkpointed
 // forward run's ends and results.
 size_t tangent_smem_bytes(unsigned rows, unsigned mm, unsigned block);
 bool tangent_world(uint32_t flags);
 cudaError_t launch_tangent(const LaunchSpec& s, const KernelArgs& a, const ce_params& p, const float* dstart,
-                           const float* dmuscle, const float* dfriction, float* dfitness);
+                           const float* dmuscle, const float* dfriction, const float* dmass, float* dfitness);
 // `mismatch` (NULL: no check): per creature, bits of reruns that did not
 // reproduce the forward run to the bit (bit 0 a segment's rerun against the
 // next checkpoint, bit 1 a substep's kept rerun against the next tape state).

@@ -28,6 +28,11 @@ struct Tangent {
     // 1/duty, 1/(1-duty), stiffness), one friction a node row; null for 0.
     const float* du_muscle;
     const float* du_friction;
+    const float* du_mass;  // one mass a node row; null for 0
+
+    // The tangents of node i's mass and inverse mass.
+    __device__ __forceinline__ float dmass(unsigned i) const { return du_mass ? du_mass[i] : 0.0f; }
+    __device__ __forceinline__ float dinv(unsigned i, float im) const { return -im * im * dmass(i); }
 
     __device__ __forceinline__ float mu_dir(unsigned k, unsigned f) const {
         return du_muscle ? du_muscle[kGradMuscle * k + f] : 0.0f;
@@ -163,7 +168,9 @@ struct Tangent {
             const float2 l0 = d.vel(i0), l1 = d.vel(i1);
             const float dwx = 0.5f * (l0.x + l1.x), dwy = 0.5f * (l0.y + l1.y);
             const float dspeed = speed > 0.0f ? (wx * dwx + wy * dwy) / speed : 0.0f;
-            const float dk = bb.x * speed <= limit ? bb.x * dspeed : 0.0f;
+            const float dlimit = du_mass ? 0.5f * C::inv_h * (dmass(i0) + dmass(i1)) : 0.0f;
+            const float dk = bb.x * speed <= limit ? bb.x * dspeed : dlimit;
+            float dfx = -wx * k_air, dfy = -wy * k_air;
             float ddfx = -(dwx * k_air + wx * dk), ddfy = -(dwy * k_air + wy * dk);
             if (b.w.has(CE_FLAG_WATER)) {
                 const float r0 = L.get(S.node + i0).z, r1 = L.get(S.node + i1).z;
@@ -183,12 +190,19 @@ struct Tangent {
                 const float sx = wx - lx, sy = wy - ly, dsx = dwx - dlx, dsy = dwy - dly;
                 const float xw = kWaterDrag * wet * ba.y * width * speed;
                 const float k_water = fminf(xw, limit);
-                const float dkw = xw <= limit ? kWaterDrag * ba.y * width * (dwet * speed + wet * dspeed) : 0.0f;
+                const float dkw = xw <= limit ? kWaterDrag * ba.y * width * (dwet * speed + wet * dspeed) : dlimit;
+                dfx -= sx * k_water + lx * k_water * kWaterAlong;
+                dfy -= sy * k_water + ly * k_water * kWaterAlong;
                 ddfx -= dsx * k_water + sx * dkw + kWaterAlong * (dlx * k_water + lx * dkw);
                 ddfy -= dsy * k_water + sy * dkw + kWaterAlong * (dly * k_water + ly * dkw);
             }
-            d.vel(i0) = make_float2(l0.x + bb.z * ddfx, l0.y + bb.z * ddfy);
-            d.vel(i1) = make_float2(l1.x + bb.w * ddfx, l1.y + bb.w * ddfy);
+            float ds0 = 0.0f, ds1 = 0.0f;
+            if (du_mass) {
+                ds0 = 0.5f * C::h * dinv(i0, L.get(S.node + i0).y);
+                ds1 = 0.5f * C::h * dinv(i1, L.get(S.node + i1).y);
+            }
+            d.vel(i0) = make_float2(l0.x + bb.z * ddfx + ds0 * dfx, l0.y + bb.z * ddfy + ds0 * dfy);
+            d.vel(i1) = make_float2(l1.x + bb.w * ddfx + ds1 * dfx, l1.y + bb.w * ddfy + ds1 * dfy);
         }
     }
 
@@ -215,6 +229,14 @@ struct Tangent {
             float2 dv = d.vel(i);
             dv.x += C::h * dfp.x * im;
             dv.y += C::h * (dfp.y + dfy) * im;
+            if (du_mass) {
+                // The world forces are a mass times an acceleration, so only
+                // the muscle force (the kept A.force entry) feels the mass.
+                const float2 F = reinterpret_cast<const float2*>(&L.base[(bw.A.force + i / 2u) * 32u])[i % 2u];
+                const float dim = dinv(i, im);
+                dv.x += C::h * F.x * dim;
+                dv.y += C::h * F.y * dim;
+            }
             if (b.w.has(CE_FLAG_AIR)) {
                 dv.x *= b.p.air_sub;
                 dv.y *= b.p.air_sub;
@@ -244,10 +266,11 @@ struct Tangent {
             const float2 l0 = d.pos(i0), l1 = d.pos(i1);
             const float ddx = l1.x - l0.x, ddy = l1.y - l0.y;
             const float dlen = len0 >= 1e-9f ? (dx * ddx + dy * ddy) / len : 0.0f;
-            const float ds = dlen * ba.y / ((w0 + w1) * len * len);
+            const float dw0 = du_mass ? dinv(i0, w0) : 0.0f, dw1 = du_mass ? dinv(i1, w1) : 0.0f;
+            const float ds = dlen * ba.y / ((w0 + w1) * len * len) - sc * (dw0 + dw1) / (w0 + w1);
             const float mx = ds * dx + sc * ddx, my = ds * dy + sc * ddy;
-            d.pos(i0) = make_float2(l0.x + w0 * mx, l0.y + w0 * my);
-            d.pos(i1) = make_float2(l1.x - w1 * mx, l1.y - w1 * my);
+            d.pos(i0) = make_float2(l0.x + w0 * mx + dw0 * sc * dx, l0.y + w0 * my + dw0 * sc * dy);
+            d.pos(i1) = make_float2(l1.x - w1 * mx - dw1 * sc * dx, l1.y - w1 * my - dw1 * sc * dy);
         }
     }
 
@@ -279,15 +302,16 @@ struct Tangent {
         dg[2] = make_float2(-(dg[0].x + dg[1].x), -(dg[0].y + dg[1].y));
     }
 
-    // Adds w_n (dlam g_n + lam dg_n) to the tangents of the three nodes.
+    // Adds w_n (dlam g_n + lam dg_n) + dw_n lam g_n to the tangents of the
+    // three nodes (w_n their inverse masses).
     template <bool VEL>
-    __device__ __forceinline__ void push_tan(const unsigned (&node)[3], const float (&wn)[3], const float2 (&gv)[3],
-                                             const float2 (&dg)[3], float lam, float dlam) const {
+    __device__ __forceinline__ void push_tan(const unsigned (&node)[3], const float (&wn)[3], const float (&dwn)[3],
+                                             const float2 (&gv)[3], const float2 (&dg)[3], float lam, float dlam) const {
         for (int n = 0; n < 3; n++) {
             float2& e = VEL ? d.vel(node[n]) : d.pos(node[n]);
             const float2 o = e;
-            e = make_float2(o.x + wn[n] * (dlam * gv[n].x + lam * dg[n].x),
-                            o.y + wn[n] * (dlam * gv[n].y + lam * dg[n].y));
+            e = make_float2(o.x + wn[n] * (dlam * gv[n].x + lam * dg[n].x) + dwn[n] * lam * gv[n].x,
+                            o.y + wn[n] * (dlam * gv[n].y + lam * dg[n].y) + dwn[n] * lam * gv[n].y);
         }
     }
 
@@ -333,15 +357,20 @@ struct Tangent {
             float2 gv[3], dg[3];
             geometry_tan(u, v, du, dv, at_head, gv, dg);
             const float wn[3] = {rb.x, rb.y, rb.z};
+            const unsigned node[3] = {tip, far, hub};
+            float dwn[3] = {0.0f, 0.0f, 0.0f};
             float wgt = 0.0f, dwgt = 0.0f;
             for (int n = 0; n < 3; n++) {
-                wgt += wn[n] * (gv[n].x * gv[n].x + gv[n].y * gv[n].y);
-                dwgt += 2.0f * wn[n] * (gv[n].x * dg[n].x + gv[n].y * dg[n].y);
+                if (du_mass) {
+                    dwn[n] = dinv(node[n], wn[n]);
+                }
+                const float gg = gv[n].x * gv[n].x + gv[n].y * gv[n].y;
+                wgt += wn[n] * gg;
+                dwgt += 2.0f * wn[n] * (gv[n].x * dg[n].x + gv[n].y * dg[n].y) + dwn[n] * gg;
             }
             const float lam = -error / wgt;
             const float dlam = -derror / wgt + error * dwgt / (wgt * wgt);
-            const unsigned node[3] = {tip, far, hub};
-            push_tan<false>(node, wn, gv, dg, lam, dlam);
+            push_tan<false>(node, wn, dwn, gv, dg, lam, dlam);
         }
     }
 
@@ -422,16 +451,21 @@ struct Tangent {
                          gv, dg);
             const unsigned node[3] = {k.tip, k.far, k.hub};
             const float wn[3] = {k.w_tip, k.w_far, k.w_hub};
+            float dwn[3] = {0.0f, 0.0f, 0.0f};
             float rate = 0.0f, drate = 0.0f, dwgt = 0.0f;
             for (int n = 0; n < 3; n++) {
+                if (du_mass) {
+                    dwn[n] = dinv(node[n], wn[n]);
+                }
                 const float2 dvn = d.vel(node[n]);
                 rate += gv[n].x * vn[n].x + gv[n].y * vn[n].y;
                 drate += dg[n].x * vn[n].x + dg[n].y * vn[n].y + gv[n].x * dvn.x + gv[n].y * dvn.y;
-                dwgt += 2.0f * wn[n] * (gv[n].x * dg[n].x + gv[n].y * dg[n].y);
+                dwgt += 2.0f * wn[n] * (gv[n].x * dg[n].x + gv[n].y * dg[n].y) +
+                        dwn[n] * (gv[n].x * gv[n].x + gv[n].y * gv[n].y);
             }
             const float lam = -share * rate / wgt;
             const float dlam = -share * drate / wgt + share * rate * dwgt / (wgt * wgt);
-            push_tan<true>(node, wn, gv, dg, lam, dlam);
+            push_tan<true>(node, wn, dwn, gv, dg, lam, dlam);
         }
     }
 
@@ -471,9 +505,17 @@ struct Tangent {
             }
         }
         // Fitness com_x = sum m x / sum m.
-        float dfit = 0.0f;
+        float dfit = 0.0f, com_x = 0.0f;
         for (unsigned i = 0u; i < r.nodes; i++) {
-            dfit += b.L.get(b.S.node + i).x * d.pos(i).x;
+            const float m = b.L.get(b.S.node + i).x;
+            dfit += m * d.pos(i).x;
+            com_x += m * b.t.pos(i).x;
+        }
+        com_x *= r.inv_mass;
+        if (du_mass) {
+            for (unsigned i = 0u; i < r.nodes; i++) {
+                dfit += dmass(i) * (b.t.pos(i).x - com_x);
+            }
         }
         return dfit * r.inv_mass;
     }
@@ -482,7 +524,7 @@ struct Tangent {
 template <class W, int RATE>
 __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, const ce_params p, const float* dstart,
                                                             const float* dmuscle, const float* dfriction,
-                                                            float* dfitness) {
+                                                            const float* dmass, float* dfitness) {
     extern __shared__ float4 smem[];
     using B = Backward<W, RATE>;
     const unsigned threads = blockDim.x;
@@ -522,7 +564,8 @@ __global__ void __launch_bounds__(kBlock, 1) tangent_kernel(const KernelArgs a, 
         if (mine != kNone) {
             const unsigned cidx = a.order ? __ldg(a.order + mine) : p.base + mine;
             const Tangent<W, RATE> tl{back, tan, dmuscle ? dmuscle + (size_t)cidx * kGradMuscle * a.mm : nullptr,
-                                      dfriction ? dfriction + (size_t)cidx * a.rows : nullptr};
+                                      dfriction ? dfriction + (size_t)cidx * a.rows : nullptr,
+                                      dmass ? dmass + (size_t)cidx * a.rows : nullptr};
             dfitness[cidx] = tl.run(cidx, dstart ? dstart + (size_t)cidx * per : nullptr);
         }
     }

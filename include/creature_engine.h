@@ -498,14 +498,15 @@ ce_status ce_tape_free(ce_tape* tape);
  * fields, on the same FP32 trajectory and contact, slip and joint-limit
  * modes as the forward run. Directions in packed order, laid out as
  * ce_backward's gradient (ce_tape_shape's rows and muscle slots), each NULL
- * for zero but not all three: `dstart` rows x 2 floats a creature (start
+ * for zero but not all four: `dstart` rows x 2 floats a creature (start
  * positions), `dmuscle` 9 x muscle slots (amplitude, hill, cap,
- * 1/capacity, phase, duty, 1/duty, 1/(1-duty), stiffness), `dfriction` rows.
+ * 1/capacity, phase, duty, 1/duty, 1/(1-duty), stiffness), `dfriction` rows,
+ * `dmass` rows (node masses, with their inverses).
  * <ce_backward's gradient, direction> equals `dfitness` up to the rounding
  * of the two derivative computations: the adjoint's check. No counterpart
  * in the reference. */
 ce_status ce_tangent(ce_tape* tape, const float* dstart, const float* dmuscle, const float* dfriction,
-                     float* dfitness);
+                     const float* dmass, float* dfitness);
 /* The forward run's checkpoints, for checking: per creature (packed order)
  * ceil(steps / 16) checkpoints of rows x 4 + muscle slots floats (positions
  * and velocities of each node row as (x, y) pairs, then the muscles' energy
