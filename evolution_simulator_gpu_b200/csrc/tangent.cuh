@@ -1,8 +1,8 @@
 // The tangent-linear run of a creature's trial (included by adjoint.cu,
 // inside its namespace, after Backward): the forward derivative of the
 // fitness along a direction of the start positions, the muscles' record
-// fields and the nodes' friction, carried substep by substep beside the
-// FP32 trajectory itself.
+// fields, the nodes' friction and the nodes' masses, carried substep by
+// substep beside the FP32 trajectory itself.
 //
 // Each substep first takes the derivative of the muscle pass from the
 // substep's start state, then runs the forward substep through

@@ -277,7 +277,8 @@ def test_checkpoints_hold_the_state_every_16_steps(engine):
 def tangent_cases(engine):
     """Per world and trial length: the backward's gradient terms and the
     tangent-linear run's d fitness along random directions of the start
-    positions, the muscle record fields and the frictions (each part alone),
+    positions, the muscle record fields, the frictions and the masses (each
+    part alone),
     and which trials count; computed once, on first use."""
     cache = {}
 
@@ -297,12 +298,14 @@ def tangent_cases(engine):
             ds = rng.normal(size=(n, rows, 2)).astype(np.float32)
             dm = rng.normal(size=(n, mm, 9)).astype(np.float32)
             df = rng.normal(size=(n, rows)).astype(np.float32)
+            dn = rng.normal(size=(n, rows)).astype(np.float32)
             for c in range(n):
-                ds[c, nodes[c]:], df[c, nodes[c]:], dm[c, muscles[c]:] = 0, 0, 0
+                ds[c, nodes[c]:], df[c, nodes[c]:], dm[c, muscles[c]:], dn[c, nodes[c]:] = 0, 0, 0, 0
             parts = {
                 "start": (tape.tangent(dstart=ds), g[:, 9 * mm + 2 * rows:9 * mm + 4 * rows] * ds.reshape(n, -1)),
                 "muscle": (tape.tangent(dmuscle=dm), g[:, :9 * mm] * dm.reshape(n, -1)),
                 "friction": (tape.tangent(dfriction=df), g[:, 9 * mm:9 * mm + rows] * df),
+                "mass": (tape.tangent(dmass=dn), g[:, 9 * mm + rows:9 * mm + 2 * rows] * dn),
             }
         cache[name, seconds] = (parts, res["fitness"] > -1e19)
         return cache[name, seconds]
@@ -310,12 +313,13 @@ def tangent_cases(engine):
     return get
 
 
-@pytest.mark.parametrize("part", ["start", "muscle", "friction"])
+@pytest.mark.parametrize("part", ["start", "muscle", "friction", "mass"])
 @pytest.mark.parametrize("seconds,share", [(16.0 / 60.0, 0.98), (20.0, 0.95)])
 @pytest.mark.parametrize("name", ["gradients", "refine", "effects"])
 def test_adjoint_equals_the_tangent_linear_run(tangent_cases, name, part, seconds, share):
     """The dot-product test of the adjoint: for a random direction u of the
-    start positions, of the muscles' record fields or of the frictions,
+    start positions, of the muscles' record fields, of the frictions or of the
+    node masses,
     <backward's gradient, u> against the tangent-linear run (ce_tangent)
     along u. Both differentiate the forward run's own FP32 trajectory with
     its contact, slip and joint-limit modes, so they differ only by the
