@@ -117,6 +117,27 @@ class PopulationC(C.Structure):
                 ("count", C.c_size_t), ("strength_scale", C.c_void_p)]
 
 
+class CmaC(C.Structure):
+    _fields_ = [("templates", PopulationC), ("exploring", C.c_void_p), ("offsets", C.c_void_p),
+                ("mean", C.c_void_p), ("covariance", C.c_void_p), ("path_c", C.c_void_p),
+                ("path_sigma", C.c_void_p), ("sigma", C.c_void_p)]
+
+
+class CmaDraw(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("generation", C.c_uint32), ("reserved", C.c_uint32), ("round", C.c_uint64),
+                ("first_id", C.c_uint64), ("strength", C.c_float), ("min_size", C.c_float),
+                ("max_size", C.c_float), ("min_friction", C.c_float), ("max_friction", C.c_float)]
+
+
+class AuditSumsC(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("sum", C.c_double * 6), ("xx", (C.c_double * 6) * 6)]
+
+
+class AuditC(C.Structure):
+    _fields_ = [("creatures", C.c_uint64), ("steps", C.c_uint64), ("stops", C.c_uint64 * 3), ("rows", C.c_uint32),
+                ("reserved", C.c_uint32), ("a", AuditSumsC * 2), ("b", AuditSumsC * 2)]
+
+
 class WavePackC(C.Structure):
     _fields_ = [("lanes", C.c_void_p), ("lanes_len", C.c_size_t), ("muscles", C.c_void_p),
                 ("muscles_len", C.c_size_t), ("heads", C.c_void_p), ("count", C.c_size_t)]
@@ -206,6 +227,14 @@ def _bind(lib: C.CDLL) -> None:
                                      P(C.c_size_t)]),
         "ce_sample_device": (C.c_int, [P(PopulationC), C.c_uint64, C.c_size_t, C.c_float, C.c_uint64, C.c_uint64,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ce_cma_offsets": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+        "ce_cma_init": (C.c_int, [P(CmaC), C.c_void_p]),
+        "ce_cma_ask": (C.c_int, [P(CmaC), P(CmaDraw), C.c_uint64, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+        "ce_cma_tell": (C.c_int, [P(CmaC), P(PopulationC), C.c_void_p, C.c_uint64, C.c_size_t, C.c_void_p]),
+        "ce_audit_scratch_bytes": (C.c_size_t, [C.c_size_t]),
+        "ce_audit_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
         "ce_dump_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World), C.c_void_p]),
         "ce_dump_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, P(World),
                                           C.c_void_p, C.c_void_p]),
@@ -250,7 +279,8 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_noalloc_scratch_bytes", "ce_forward", "ce_tape_results", "ce_tape_grad_floats", "ce_tape_shape",
             "ce_tape_seconds", "ce_backward", "ce_backward_checked", "ce_tape_free", "ce_tangent", "ce_gene_gradients", "ce_tape_checkpoints",
             "ce_replay_decode", "ce_sample_rows", "ce_sample_device", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
-            "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune"]
+            "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune", "ce_cma_offsets", "ce_cma_init",
+            "ce_cma_ask", "ce_cma_tell", "ce_audit_scratch_bytes", "ce_audit_device"]
 
 
 def _check(status: int, what: str) -> None:
@@ -959,6 +989,41 @@ def shape_classes(pop: Population, wave: "WavePack", indices=None, global_layout
     _check(lib().ce_shape_classes(C.byref(pc), _ptr(idx), len(wave), _ptr(wave.slots), 1 if global_layout else 0,
                                   _ptr(out)), "ce_shape_classes")
     return out
+
+
+def audit(results: np.ndarray, pop: "Population", bars: np.ndarray, a_cap: int = 1 << 16, device=None) -> dict:
+    """The rung audit of a batch on the GPU (ce_audit_device): `results` in
+    population order, `pop` the batch's genomes (flags, first muscle's
+    period), bars[i] the screen bar of creature i's block (NaN: none).
+    Returns Audit::note's tallies, the audit row count and, per rung, class
+    A and class B sums and class A's feature words."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+
+    def up(arr):
+        return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(dev)
+
+    n = len(results)
+    L = lib()
+    dr, dg, dm = up(results), up(pop.genomes), up(pop.muscles if len(pop.muscles) else np.zeros(1, MUSCLE_DTYPE))
+    db = up(np.ascontiguousarray(bars, np.float32))
+    scratch = torch.empty(int(L.ce_audit_scratch_bytes(n)), dtype=torch.uint8, device=dev)
+    out = torch.empty(C.sizeof(AuditC), dtype=torch.uint8, device=dev)
+    words = torch.empty(2 * a_cap * 6, dtype=torch.int16, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    _check(L.ce_audit_device(dr.data_ptr(), dg.data_ptr(), dm.data_ptr(), db.data_ptr(), n, scratch.data_ptr(),
+                             scratch.numel(), out.data_ptr(), words.data_ptr(), a_cap, stream.cuda_stream),
+           "ce_audit_device")
+    stream.synchronize()
+    a = AuditC.from_buffer_copy(out.cpu().numpy().tobytes())
+
+    def sums(s):
+        return int(s.n), list(s.sum), [list(row) for row in s.xx]
+
+    w = words.cpu().numpy().view(np.uint16).reshape(2, a_cap, 6)
+    return dict(creatures=int(a.creatures), steps=int(a.steps), stops=list(a.stops), rows=int(a.rows),
+                sums=[[sums(a.a[r]), sums(a.b[r])] for r in range(2)],
+                a_words=[w[r, :min(int(a.a[r].n), a_cap)].copy() for r in range(2)])
 
 
 def height_bin_edges() -> np.ndarray:

@@ -35,11 +35,11 @@ NVCC_FLAGS = [
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp"]
 
 CUDA_SOURCES = ["advance.cu", "adjoint.cu", "bucket.cu", "engine.cu", "metrics.cu", "peak.cu", "noalloc.cu",
-                "sample.cu", "pack.cu"]
-# The device packer, gene gradients and ascent step round as their host
-# counterparts: IEEE division and square root, no contraction of
-# multiply-adds.
-IEEE_SOURCES = {"pack.cu"}
+                "sample.cu", "pack.cu", "cma.cu", "audit.cu"]
+# The device packer, gene gradients and ascent step, the CMA-ES emitters and
+# the rung audit's sums round as their host counterparts: IEEE division and
+# square root, no contraction of multiply-adds.
+IEEE_SOURCES = {"pack.cu", "cma.cu", "audit.cu"}
 
 
 def file_flags(name: str) -> list[str]:

@@ -271,7 +271,8 @@ def _evaluate(engine, pop, world, chunk: int):
 def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sigma: float = 0.05,
            elites: int = 16_384, steps: int = 5, step: float = 1e-2, seed: int = 4, chunk: int = 2_000_000,
            resample: bool = True, rank: int = 0, world_size: int = 1, group=None, device=None,
-           sampler: str = "host", guided: bool = False, ascent: str = "device", line_search=()) -> dict:
+           sampler: str = "host", guided: bool = False, ascent: str = "device", line_search=(),
+           cma_samples: int = 0) -> dict:
     """One gradient-refined search generation and its resampling yardstick.
 
     1. `count` samples of `parents` parents (σ = sigma), evaluated in one
@@ -302,7 +303,12 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
     runs `steps` ascent steps whose size each creature chooses: per step one
     gradient (checkpointed forward and backward run), then one evaluation of
     each factor's step, and each creature moves to its best candidate if
-    that beats where it stands; its GPU time counts every evaluation."""
+    that beats where it stands; its GPU time counts every evaluation. With
+    `cma_samples` > 0, a further arm gives every elite a separable CMA-ES
+    optimizer (the reference's optimizer emitter, cma.CmaEmitters, its
+    ask and tell on the GPU) and runs generations of `cma_samples` samples
+    an elite for about the same GPU time, ask and tell kernels included;
+    each elite keeps the best of itself and its optimizer's samples."""
     draw = samples if sampler == "host" else samples_gpu
     report = dict(parents=parents, samples=count, sigma=sigma, elites=elites, steps=steps, step=step,
                   ranks=world_size, sampler=sampler, ascent=ascent)
@@ -431,6 +437,15 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
         report["line"] = dict(factors=list(line_search), gpu_s=tl[2], mean_best=tl[0] / n_el, gain=gain_l,
                               gain_per_gpu_s=gain_l / max(tl[2], 1e-12), improved=tl[1] / n_el,
                               host_s=time.perf_counter() - t0)
+    if cma_samples and len(mine):
+        report["cma"] = _cma_arm(engine, world, elite, f0, cma_samples, refine_s, seed, rank, chunk,
+                                 (spec.friction_lo, spec.friction_hi))
+        tc = shard.all_sum([report["cma"].pop("best_sum"), report["cma"]["improved"], report["cma"]["gpu_s"],
+                            report["cma"]["generations"]], world_size, group, device)
+        gain_c = (tc[0] - tot[1]) / n_el
+        report["cma"].update(gpu_s=tc[2], mean_best=tc[0] / n_el, gain=gain_c,
+                             gain_per_gpu_s=gain_c / max(tc[2], 1e-12), improved=tc[1] / n_el,
+                             generations=tc[3] / world_size)
     if guided:
         t0 = time.perf_counter()
         if stepped is None:
@@ -443,3 +458,38 @@ def search(engine, spec, world, parents: int = 1024, count: int = 1_000_000, sig
                                 gain=gain_g, gain_per_gpu_s=gain_g / max(tg[2], 1e-12), improved=tg[1] / n_el,
                                 host_s=time.perf_counter() - t0)
     return report
+
+
+def _cma_arm(engine, world, elite: api.Population, f0: np.ndarray, per: int, budget: float, seed: int, rank: int,
+             chunk: int, friction) -> dict:
+    """Generations of a CMA-ES optimizer per elite until `budget` GPU
+    seconds are spent (evaluations, asks and tells); `friction` is the
+    range repair holds frictions to (the workload's). Returns this rank's
+    sum of best fitness, the count improved, GPU seconds and generations."""
+    import torch
+    from .cma import CmaEmitters
+    t0 = time.perf_counter()
+    opt = CmaEmitters(elite)
+    E = len(elite)
+    best = f0.astype(np.float64).copy()
+    secs, gens, kernel_s = 0.0, 0, 0.0
+    owner = np.arange(per * E) % E
+    while secs < budget:
+        genes, _ = opt.ask_device(per * E, seed=seed + 3, generation=gens, round=rank, first=0, friction=friction)
+        kids = opt.download(genes)
+        # Samples keep their elite's id, so they see its tremor phase.
+        kids.genomes["id"] = elite.genomes["id"][owner]
+        fk, busy = _evaluate(engine, kids, world, chunk)
+        # The samples' genes are still on the device: tell reads them there.
+        keys = torch.as_tensor(fk).to(opt.device)
+        opt.tell_device(genes[:3] + genes[4:], keys, 0, per * E)
+        ks = opt.kernel_seconds()
+        secs += busy + ks
+        kernel_s += ks
+        gens += 1
+        np.maximum.at(best, owner, np.where(fk > -1e19, fk, -np.inf).astype(np.float64))
+    sig = opt.sigma.cpu().numpy()
+    return dict(samples_per_generation=per, generations=gens, gpu_s=secs, ask_tell_gpu_s=kernel_s,
+                best_sum=float(best.sum()),
+                improved=float((best > f0).sum()), sigma_median=float(np.median(sig)),
+                host_s=time.perf_counter() - t0)

@@ -361,6 +361,104 @@ ce_status ce_niche_batch(const ce_population* pop, const uint32_t* indices, size
 int64_t ce_niche(const ce_node_gene* nodes, uint32_t node_count, uint32_t muscle_count,
                  const ce_metrics* m, int global_layout, uint8_t niche_out[6]);
 
+/* ---- CMA-ES emitters on the device ---- */
+/* One emitter per template body: the reference's CmaEmitter (src/qd.rs:
+ * 2130-2188), which the reference keeps on the host, in either of its modes:
+ * a separable CMA-ES optimizer (CmaEmitter::optimizer: the parameter vector
+ * of write_parameters, src/qd.rs:2734-2770, in physical units) or a CMA-ME
+ * emitter (CmaEmitter::new: exploring_parameters, src/qd.rs:2504-2538,
+ * normalised to about 0-1). Every pointer is a device address. `templates`
+ * holds one template body an emitter (count = emitters, genes packed in
+ * order from row 0); emitter e's coordinates are [offsets[e], offsets[e + 1])
+ * of mean, covariance, path_c and path_sigma, and sigma[e] is its step
+ * size. */
+typedef struct ce_cma {
+    ce_population templates;
+    const uint8_t* exploring; /* 1 a CMA-ME emitter, 0 an optimizer, one an emitter; NULL: all optimizers */
+    const uint64_t* offsets;  /* emitters + 1 entries (ce_cma_offsets) */
+    float* mean;
+    float* covariance;
+    float* path_c;
+    float* path_sigma;
+    float* sigma;             /* one an emitter */
+} ce_cma;
+/* What a batch of samples is drawn with. Sample g draws from the breeding
+ * stream Rng::stream(seed, generation, round, slot g) (src/evolution.rs:
+ * 455-600): the reference's counter-based generator, restated, so a sample
+ * is the reference's child for that ring slot given the same emitter state. */
+typedef struct ce_cma_draw {
+    uint64_t seed;                    /* Config::seed */
+    uint32_t generation;
+    uint32_t reserved;                /* 0 */
+    uint64_t round;                   /* the breeding round */
+    uint64_t first_id;                /* sample g gets id first_id + g */
+    float strength;                   /* Config::mutation (1 by default) */
+    float min_size, max_size;         /* repair's diameter range (0.06, 0.12 m by default) */
+    float min_friction, max_friction; /* repair's friction range (0.65, 1 by default) */
+} ce_cma_draw;
+/* The coordinate offsets of emitters with these template genomes and modes
+ * (host arrays; `exploring` may be NULL; `offsets` gets emitters + 1
+ * entries, the last the total). */
+ce_status ce_cma_offsets(const ce_genome* templates, const uint8_t* exploring, size_t emitters,
+                         uint64_t* offsets);
+/* CmaEmitter::optimizer and CmaEmitter::new: the means at the templates'
+ * coordinates, unit covariances, zero paths, step size 0.5 for an optimizer
+ * and 0.12 for a CMA-ME emitter. */
+ce_status ce_cma_init(const ce_cma* cma, void* stream);
+/* sample_optimizing / sample_exploring (src/qd.rs:2244-2289, 2377-2402) for
+ * samples [first, first + count): sample g belongs to emitter g mod emitters,
+ * goes back to genes with apply_parameters / apply_exploring_parameters
+ * (src/qd.rs:2579-2606, 2773-2811) and repair's diameter and friction
+ * ranges (src/evolution.rs:1230-1234), id draw->first_id + g. The rows are
+ * laid out as ce_sample_device lays them (ce_sample_rows with the templates
+ * as parents sizes them); `strength_out` (or NULL) gets the templates'
+ * strength factors, `values` (or NULL) the drawn coordinates, `stride`
+ * floats a sample. */
+ce_status ce_cma_ask(const ce_cma* cma, const ce_cma_draw* draw, uint64_t first, size_t count,
+                     ce_node_gene* nodes, ce_bone_gene* bones, ce_muscle_gene* muscles, float* strength_out,
+                     ce_genome* genomes, float* values, size_t stride, void* stream);
+/* tell, tell_optimizing and tell_exploring (src/qd.rs:2213-2243,
+ * 2290-2376, 2405-2474) from the samples [first, first + count) of one
+ * ce_cma_ask (their genes and one key a sample, in that order: fitness for
+ * an optimizer, the archive's improvement key for a CMA-ME emitter): each
+ * emitter keeps its finite samples above the failure score whose body plan
+ * is the template's (counts and bone and muscle connections, gene by gene),
+ * the best 1024 best first (ties by sample index), and updates its mean,
+ * paths, covariance and step size. At most 4096 samples an emitter a call. */
+ce_status ce_cma_tell(const ce_cma* cma, const ce_population* samples, const float* keys, uint64_t first,
+                      size_t count, void* stream);
+
+/* ---- rung audit on the device ---- */
+/* Sums::add's sums of one class of feature vectors (src/rungs.rs:286-299):
+ * the count, the sum of each feature and of each product, float64. */
+typedef struct ce_audit_sums {
+    uint64_t n;
+    double sum[6];
+    double xx[6][6];
+} ce_audit_sums;
+/* One batch's rung audit: Audit::note over every trial (src/rungs.rs:
+ * 510-525) and GenAudit::of over its audit rows (src/rungs.rs:319-345). */
+typedef struct ce_audit {
+    uint64_t creatures, steps;
+    uint64_t stops[3];       /* stopped by R1, R2 and the 5 s screen */
+    uint32_t rows, reserved; /* audit rows (GenAudit::rows) */
+    ce_audit_sums a[2], b[2]; /* per rung: class A (reached the 5 s bar), class B */
+} ce_audit;
+/* Scratch ce_audit_device needs for `count` trials. */
+size_t ce_audit_scratch_bytes(size_t count);
+/* The rung audit of `count` trials from resident results, in batch order
+ * (record_rungs, src/storage.rs:672-708): creature i's result, genome (its
+ * flags: rungs::AUDIT and EXEMPT; its first muscle's period, from `muscles`)
+ * and its block's screen bar bars[i] (not finite: no bar). Audit rows are
+ * the trials of AUDIT creatures whose trace is not empty; every float64 sum
+ * is added in row order, as the reference adds it. a_words (or NULL) gets,
+ * per rung r, class A's feature words (6 halves a row) at
+ * [(r a_cap + i) 6], the first a_cap rows. All pointers are device
+ * addresses; scratch holds ce_audit_scratch_bytes(count) bytes. */
+ce_status ce_audit_device(const ce_result* results, const ce_genome* genomes, const ce_muscle_gene* muscles,
+                          const float* bars, size_t count, void* scratch, size_t scratch_bytes, ce_audit* out,
+                          uint16_t* a_words, size_t a_cap, void* stream);
+
 /* ---- engine ------------------------------------------------------------ */
 typedef struct ce_engine ce_engine;
 

@@ -61,6 +61,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--sampler", default="device", choices=["device", "host"], help="where the samples are drawn")
     ap.add_argument("--line-search", default="", help="step-size factors of a line-search ascent arm, e.g. 0.25,1,4,16")
+    ap.add_argument("--cma", type=int, default=0, help="samples an elite a generation of a CMA-ES arm (0: no arm)")
     args = ap.parse_args()
     if args.generations:
         return generations(args)
@@ -108,7 +109,8 @@ def refined(args) -> None:
             out = refine.search(eng, w.spec, w.world(duration=args.seconds), parents=args.parents,
                                 count=args.creatures, elites=args.elites, steps=args.steps, sampler=args.sampler,
                                 guided=True, rank=rank, world_size=world_size, device=device,
-                                line_search=tuple(float(f) for f in args.line_search.split(",") if f))
+                                line_search=tuple(float(f) for f in args.line_search.split(",") if f),
+                                cma_samples=args.cma)
     finally:
         if world_size > 1:
             dist.destroy_process_group()

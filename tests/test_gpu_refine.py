@@ -1,7 +1,7 @@
 """A small gradient-refined search generation on the GPU (refine.search):
 the checkpointed forward run scores the elites exactly as the batched
-evaluation did, both arms keep each elite's best fitness, and the report
-carries GPU times and gains."""
+evaluation did, every arm (resampling, guided, CMA-ES) keeps each elite's
+best fitness, and the report carries GPU times and gains."""
 import numpy as np
 import pytest
 
@@ -14,10 +14,11 @@ pytestmark = pytest.mark.gpu
 def test_small_refined_search(engine):
     w = WORKLOADS["refine"]
     rep = refine.search(engine, w.spec, w.world(duration=1.0), parents=32, count=4096, elites=256, steps=2,
-                        guided=True)
-    r, s, g = rep["refine"], rep["resample"], rep["guided"]
+                        guided=True, cma_samples=8)
+    r, s, g, c = rep["refine"], rep["resample"], rep["guided"], rep["cma"]
     assert r["first_equal"] is True
     assert np.isfinite(rep["elite_mean_fitness"])
-    for arm in (r, s, g):
+    assert c["generations"] >= 1 and np.float32(0.01) <= c["sigma_median"] <= 30
+    for arm in (r, s, g, c):
         assert arm["gpu_s"] > 0 and arm["gain"] >= 0 and np.isfinite(arm["gain_per_gpu_s"])
     assert s["children_per_elite"] >= 1
