@@ -27,8 +27,9 @@ namespace {
 constexpr uint32_t kAudit = 1u, kExempt = 2u;  // rungs::AUDIT, rungs::EXEMPT (src/rungs.rs:18-22)
 constexpr unsigned kFeatures = 6u;
 constexpr unsigned kTile = 256u;                 // threads of the count and write kernels
-constexpr unsigned kSumThreads = 2u * 2u * (1u + kFeatures + kFeatures * kFeatures);  // 172
-constexpr unsigned kChunk = 256u;                // rows staged at a time
+constexpr unsigned kColumns = 1u + kFeatures + kFeatures * kFeatures;  // count, sums, products: 43
+constexpr unsigned kGroup = 64u;                 // threads a (rung, class) group of the sum kernel
+constexpr unsigned kChunk = 4u * kGroup;         // rows staged at a time: one a thread
 
 __device__ __forceinline__ uint32_t bits(float f) { return __float_as_uint(f); }
 
@@ -132,18 +133,38 @@ __global__ void __launch_bounds__(kTile) audit_count_kernel(const Inputs in, uin
     }
 }
 
-// Exclusive offsets of the tiles' rows (one thread: a few thousand tiles at
-// most), and the batch's totals.
-__global__ void audit_scan_kernel(uint32_t* tile_rows, unsigned tiles, size_t count, ce_audit* out) {
-    if (threadIdx.x != 0u || blockIdx.x != 0u) return;
-    uint32_t at = 0u;
-    for (unsigned b = 0u; b < tiles; b++) {
-        const uint32_t n = tile_rows[b];
-        tile_rows[b] = at;
-        at += n;
+// Exclusive offsets of the tiles' rows and the batch's totals: one block of
+// 1024 threads, two tiles a thread (at most 2048 tiles).
+constexpr unsigned kMaxTiles = 2048u;
+__global__ void __launch_bounds__(1024) audit_scan_kernel(uint32_t* tile_rows, unsigned tiles, size_t count,
+                                                           ce_audit* out) {
+    __shared__ uint32_t warp_sum[32];
+    const unsigned t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const uint32_t x0 = 2u * t < tiles ? tile_rows[2u * t] : 0u, x1 = 2u * t + 1u < tiles ? tile_rows[2u * t + 1u] : 0u;
+    const uint32_t mine = x0 + x1;
+    uint32_t incl = mine;
+    for (unsigned d = 1u; d < 32u; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
     }
-    out->rows = at;
-    out->creatures = count;
+    if (lane == 31u) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0u) {
+        uint32_t w = warp_sum[lane], wi = w;
+        for (unsigned d = 1u; d < 32u; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+            if (lane >= d) wi += y;
+        }
+        warp_sum[lane] = wi - w;  // exclusive
+        if (lane == 31u) {
+            out->rows = wi;
+            out->creatures = count;
+        }
+    }
+    __syncthreads();
+    const uint32_t before = warp_sum[warp] + incl - mine;
+    if (2u * t < tiles) tile_rows[2u * t] = before;
+    if (2u * t + 1u < tiles) tile_rows[2u * t + 1u] = before + x0;
 }
 
 // Each tile writes its rows' indices in order: a block-wide ordered
@@ -174,23 +195,32 @@ __global__ void __launch_bounds__(kTile) audit_write_kernel(const Inputs in, con
     }
 }
 
-// GenAudit::of over the compacted rows, in order. Thread t < 172 owns one
-// column: rung r = t / 86, class k = (t / 43) % 2, moment m = t % 43 (0 the
-// count, 1-6 the sums, 7-42 the products, row-major).
-__global__ void __launch_bounds__(192) audit_sum_kernel(const Inputs in, const uint32_t* row_index, ce_audit* out,
-                                                        uint16_t* a_words, size_t a_cap) {
-    __shared__ float feat[kChunk][2][kFeatures];
-    __shared__ uint8_t cls[kChunk][2];  // 0 class A, 1 class B, 2 neither
-    const unsigned t = threadIdx.x;
-    const unsigned r = t / 86u, k = (t / 43u) % 2u, m = t % 43u;
+// GenAudit::of over the compacted rows, in order. Four groups of 64
+// threads, one a (rung, class): per chunk of 256 rows each row's features
+// are staged once as float64 (with a constant 1 in slot 6), each group gets
+// the chunk's rows of its class in row order, and thread c < 43 of a group
+// adds its column over them: c = 0 the count, 1-6 feature c - 1 times the
+// constant 1 (an exact product, so the sum is Sums::add's), 7-42 the product
+// of features (c - 7) / 6 and (c - 7) % 6. Every column is one row-ordered
+// chain of float64 multiply and add, with no branch on the row.
+__global__ void __launch_bounds__(kChunk) audit_sum_kernel(const Inputs in, const uint32_t* row_index, ce_audit* out,
+                                                           uint16_t* a_words, size_t a_cap) {
+    __shared__ double feat[kChunk][2][kFeatures + 1u];
+    __shared__ uint16_t list[4][kChunk];
+    __shared__ unsigned warp_count[4][kChunk / 32u], list_len[4];
+    const unsigned t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const unsigned group = t / kGroup, col = t % kGroup, r = group >> 1, k = group & 1u;
+    const unsigned fa = col == 0u ? kFeatures : (col <= kFeatures ? col - 1u : (col - 1u - kFeatures) / kFeatures);
+    const unsigned fb = col <= kFeatures ? kFeatures : (col - 1u - kFeatures) % kFeatures;
     const uint32_t rows = out->rows;
     double acc = 0.0;
     unsigned long long n = 0ull;
     for (uint32_t start = 0u; start < rows; start += kChunk) {
         const uint32_t len = min(kChunk, rows - start);
-        __syncthreads();
-        for (uint32_t q = t; q < len; q += blockDim.x) {
-            const uint32_t i = row_index[start + q];
+        __syncthreads();  // the last chunk's lists and features are read
+        unsigned cls[2] = {2u, 2u};  // per rung: 0 class A, 1 class B, 2 neither
+        if (t < len) {
+            const uint32_t i = row_index[start + t];
             const ce_result& res = in.results[i];
             const Trace tr(res);
             const ce_genome& g = in.genomes[i];
@@ -204,39 +234,65 @@ __global__ void __launch_bounds__(192) audit_sum_kernel(const Inputs in, const u
                                             half_of(tr.w[4u + rr], false), half_of(tr.w[6], rr == 1u),
                                             half_of(tr.w[4u + rr], true), ph};
                 bool finite = true;
-                for (unsigned a = 0u; a < kFeatures; a++) {
-                    feat[q][rr][a] = f[a];
-                    finite = finite && isfinite(f[a]);
+#pragma unroll
+                for (unsigned x = 0u; x < kFeatures; x++) {
+                    feat[t][rr][x] = (double)f[x];
+                    finite = finite && isfinite(f[x]);
                 }
+                feat[t][rr][kFeatures] = 1.0;
                 // rungs::RUNG_STEPS: R1 at step 60, R2 at 150.
-                cls[q][rr] = (counted && tr.steps() > (rr == 0u ? 60u : 150u) && finite) ? (pass3 ? 0u : 1u) : 2u;
+                cls[rr] = (counted && tr.steps() > (rr == 0u ? 60u : 150u) && finite) ? (pass3 ? 0u : 1u) : 2u;
             }
+        }
+        // Each group's rows in row order: a ballot a warp, then the warps'
+        // counts before this one.
+        unsigned ballot[4];
+#pragma unroll
+        for (unsigned q = 0u; q < 4u; q++) {
+            ballot[q] = __ballot_sync(0xffffffffu, cls[q >> 1] == (q & 1u));
+            if (lane == 0u) warp_count[q][warp] = __popc(ballot[q]);
         }
         __syncthreads();
-        if (t < kSumThreads) {
-            for (uint32_t q = 0u; q < len; q++) {
-                if (cls[q][r] != k) continue;
-                const float* f = feat[q][r];
-                if (m == 0u) {
-                    if (k == 0u && n < a_cap && a_words) {
-                        uint16_t* w = a_words + ((size_t)r * a_cap + n) * kFeatures;
-                        for (unsigned a = 0u; a < kFeatures; a++) w[a] = (uint16_t)float_to_half(f[a]);
-                    }
-                    n += 1ull;
-                } else if (m <= kFeatures) {
-                    acc += (double)f[m - 1u];
-                } else {
-                    const unsigned a = (m - 1u - kFeatures) / kFeatures, b = (m - 1u - kFeatures) % kFeatures;
-                    acc += (double)f[a] * (double)f[b];
+#pragma unroll
+        for (unsigned q = 0u; q < 4u; q++) {
+            if ((ballot[q] >> lane) & 1u) {
+                unsigned before = 0u;
+                for (unsigned v = 0u; v < warp; v++) before += warp_count[q][v];
+                list[q][before + __popc(ballot[q] & ((1u << lane) - 1u))] = (uint16_t)t;
+            }
+        }
+        if (t < 4u) {
+            unsigned all = 0u;
+            for (unsigned v = 0u; v < kChunk / 32u; v++) all += warp_count[t][v];
+            list_len[t] = all;
+        }
+        __syncthreads();
+        const unsigned L = list_len[group];
+        if (col < kColumns) {
+            if (col > 0u) {
+#pragma unroll 4
+                for (unsigned j = 0u; j < L; j++) {
+                    const unsigned q = list[group][j];
+                    acc += feat[q][r][fa] * feat[q][r][fb];
+                }
+            }
+            if (k == 0u && a_words) {
+                // Class A's feature words, the group's threads sharing the rows.
+                for (unsigned j = col; j < L; j += kColumns) {
+                    if (n + j >= a_cap) break;
+                    const unsigned q = list[group][j];
+                    uint16_t* w = a_words + ((size_t)r * a_cap + n + j) * kFeatures;
+                    for (unsigned x = 0u; x < kFeatures; x++) w[x] = (uint16_t)float_to_half((float)feat[q][r][x]);
                 }
             }
         }
+        n += L;
     }
-    if (t < kSumThreads) {
+    if (col < kColumns) {
         ce_audit_sums& s = k == 0u ? out->a[r] : out->b[r];
-        if (m == 0u) s.n = n;
-        else if (m <= kFeatures) s.sum[m - 1u] = acc;
-        else s.xx[(m - 1u - kFeatures) / kFeatures][(m - 1u - kFeatures) % kFeatures] = acc;
+        if (col == 0u) s.n = n;
+        else if (col <= kFeatures) s.sum[col - 1u] = acc;
+        else s.xx[(col - 1u - kFeatures) / kFeatures][(col - 1u - kFeatures) % kFeatures] = acc;
     }
 }
 
@@ -273,9 +329,9 @@ extern "C" ce_status ce_audit_device(const ce_result* results, const ce_genome* 
     Inputs in{results, genomes, muscles, bars, count, (count + tiles - 1u) / tiles};
     if (in.tile == 0u) in.tile = 1u;
     audit_count_kernel<<<tiles, kTile, 0, st>>>(in, tile_rows, out);
-    audit_scan_kernel<<<1, 32, 0, st>>>(tile_rows, tiles, count, out);
+    audit_scan_kernel<<<1, 1024, 0, st>>>(tile_rows, tiles, count, out);
     audit_write_kernel<<<tiles, kTile, 0, st>>>(in, tile_rows, row_index);
-    audit_sum_kernel<<<1, 192, 0, st>>>(in, row_index, out, a_words, a_cap);
+    audit_sum_kernel<<<1, kChunk, 0, st>>>(in, row_index, out, a_words, a_cap);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         ce::set_error(std::string("ce_audit_device: launch: ") + cudaGetErrorString(e));

@@ -247,8 +247,6 @@ __global__ void cma_init_kernel(const Emitters em) {
 struct AskArgs {
     ce_cma_draw draw;
     uint64_t first;
-    uint64_t tn, tb, tm;              // the templates' rows
-    uint64_t base_n, base_b, base_m;  // global row of the first sample's first row
     ce_node_gene* nodes;
     ce_bone_gene* bones;
     ce_muscle_gene* muscles;
@@ -265,13 +263,20 @@ struct AskArgs {
 __global__ void cma_ask_kernel(const Emitters em, const AskArgs a, size_t count) {
     const uint64_t E = em.t.count;
     const ce_cma_draw& w = a.draw;
+    // The templates' rows (packed from row 0, so the last one ends them) and
+    // the global row of the call's first sample, which starts its outputs.
+    const ce_genome last = em.t.genomes[E - 1u], f = em.t.genomes[a.first % E];
+    const uint64_t tn = last.node_start + last.node_count, tb = last.bone_start + last.bone_count,
+                   tm = last.muscle_start + last.muscle_count;
+    const uint64_t base_n = (a.first / E) * tn + f.node_start, base_b = (a.first / E) * tb + f.bone_start,
+                   base_m = (a.first / E) * tm + f.muscle_start;
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < count; c += (size_t)gridDim.x * blockDim.x) {
         const uint64_t g = a.first + c, e = g % E, k = g / E;
         const ce_genome tg = em.t.genomes[e];
         ce_genome o = tg;
-        o.node_start = (uint32_t)(k * a.tn + tg.node_start - a.base_n);
-        o.bone_start = (uint32_t)(k * a.tb + tg.bone_start - a.base_b);
-        o.muscle_start = (uint32_t)(k * a.tm + tg.muscle_start - a.base_m);
+        o.node_start = (uint32_t)(k * tn + tg.node_start - base_n);
+        o.bone_start = (uint32_t)(k * tb + tg.bone_start - base_b);
+        o.muscle_start = (uint32_t)(k * tm + tg.muscle_start - base_m);
         o.id = w.first_id + g;
         a.genomes[c] = o;
         const Layout l = Layout::of(tg, em.t.bones, em.explores(e));
@@ -309,7 +314,7 @@ __global__ void cma_ask_kernel(const Emitters em, const AskArgs a, size_t count)
                 else if ((node && d % 4u == 1u) || f == 2u || f == 3u) x = fmaxf(value, 0.0f);
                 else x = clampf(value, 0.0f, 1.0f);
             }
-            if (a.values) a.values[c * a.stride + d] = x;
+            if (a.values && d < a.stride) a.values[c * a.stride + d] = x;
             return x;
         };
         const ce_muscle_gene* tm = em.t.muscles + tg.muscle_start;
@@ -650,7 +655,29 @@ extern "C" ce_status ce_cma_init(const ce_cma* cma, void* stream) {
         ce::set_error("ce_cma_init: null argument or no emitters");
         return CE_ERR_INVALID;
     }
-    cma_init_kernel<<<grid_for(cma->templates.count), 256, 0, static_cast<cudaStream_t>(stream)>>>(emitters_of(cma));
+    // The templates' genes must be packed in order from row 0: ask derives
+    // every sample's rows from that (checked here, once).
+    const size_t E = cma->templates.count;
+    std::vector<ce_genome> hg(E);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(hg.data(), cma->templates.genomes, E * sizeof(ce_genome), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        ce::set_error(std::string("ce_cma_init: reading the templates: ") + cudaGetErrorString(e));
+        return CE_ERR_DEVICE;
+    }
+    uint64_t at[3] = {0, 0, 0};
+    for (size_t q = 0; q < E; q++) {
+        const ce_genome& g = hg[q];
+        if (g.node_start != at[0] || g.bone_start != at[1] || g.muscle_start != at[2]) {
+            ce::set_error("ce_cma_init: the templates' genes must be packed in order from row 0");
+            return CE_ERR_INVALID;
+        }
+        at[0] += g.node_count;
+        at[1] += g.bone_count;
+        at[2] += g.muscle_count;
+    }
+    cma_init_kernel<<<grid_for(E), 256, 0, st>>>(emitters_of(cma));
     return launched("ce_cma_init");
 }
 
@@ -666,44 +693,10 @@ extern "C" ce_status ce_cma_ask(const ce_cma* cma, const ce_cma_draw* draw, uint
         ce::set_error("ce_cma_ask: an empty diameter or friction range");
         return CE_ERR_INVALID;
     }
-    const size_t E = cma->templates.count;
-    std::vector<ce_genome> hg(E);
-    std::vector<uint8_t> mode(E, 0);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemcpyAsync(hg.data(), cma->templates.genomes, E * sizeof(ce_genome), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && cma->exploring)
-        e = cudaMemcpyAsync(mode.data(), cma->exploring, E, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        ce::set_error(std::string("ce_cma_ask: reading the templates: ") + cudaGetErrorString(e));
-        return CE_ERR_DEVICE;
-    }
-    uint64_t at[3] = {0, 0, 0};
-    for (size_t p = 0; p < E; p++) {
-        const ce_genome& g = hg[p];
-        if (g.node_start != at[0] || g.bone_start != at[1] || g.muscle_start != at[2]) {
-            ce::set_error("ce_cma_ask: the templates' genes must be packed in order from row 0");
-            return CE_ERR_INVALID;
-        }
-        if (values && dims_of(g, mode[p] != 0) > stride) {
-            ce::set_error("ce_cma_ask: `stride` is smaller than an emitter's coordinates");
-            return CE_ERR_INVALID;
-        }
-        at[0] += g.node_count;
-        at[1] += g.bone_count;
-        at[2] += g.muscle_count;
-    }
     if (count == 0) return CE_OK;
     AskArgs a;
     a.draw = *draw;
     a.first = first;
-    a.tn = at[0];
-    a.tb = at[1];
-    a.tm = at[2];
-    const ce_genome& f = hg[first % E];
-    a.base_n = (first / E) * a.tn + f.node_start;
-    a.base_b = (first / E) * a.tb + f.bone_start;
-    a.base_m = (first / E) * a.tm + f.muscle_start;
     a.nodes = nodes;
     a.bones = bones;
     a.muscles = muscles;
@@ -711,6 +704,7 @@ extern "C" ce_status ce_cma_ask(const ce_cma* cma, const ce_cma_draw* draw, uint
     a.genomes = genomes;
     a.values = values;
     a.stride = stride;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     cma_ask_kernel<<<grid_for(count), 256, 0, st>>>(emitters_of(cma), a, count);
     return launched("ce_cma_ask");
 }

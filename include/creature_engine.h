@@ -403,7 +403,9 @@ ce_status ce_cma_offsets(const ce_genome* templates, const uint8_t* exploring, s
                          uint64_t* offsets);
 /* CmaEmitter::optimizer and CmaEmitter::new: the means at the templates'
  * coordinates, unit covariances, zero paths, step size 0.5 for an optimizer
- * and 0.12 for a CMA-ME emitter. */
+ * and 0.12 for a CMA-ME emitter. Checks (reading the template genomes back,
+ * synchronising `stream`) that their genes are packed in order from row 0,
+ * which ask relies on; ask and tell only launch. */
 ce_status ce_cma_init(const ce_cma* cma, void* stream);
 /* sample_optimizing / sample_exploring (src/qd.rs:2244-2289, 2377-2402) for
  * samples [first, first + count): sample g belongs to emitter g mod emitters,
@@ -413,7 +415,8 @@ ce_status ce_cma_init(const ce_cma* cma, void* stream);
  * laid out as ce_sample_device lays them (ce_sample_rows with the templates
  * as parents sizes them); `strength_out` (or NULL) gets the templates'
  * strength factors, `values` (or NULL) the drawn coordinates, `stride`
- * floats a sample. */
+ * floats a sample (the largest emitter's coordinates; any past `stride`
+ * are not written). */
 ce_status ce_cma_ask(const ce_cma* cma, const ce_cma_draw* draw, uint64_t first, size_t count,
                      ce_node_gene* nodes, ce_bone_gene* bones, ce_muscle_gene* muscles, float* strength_out,
                      ce_genome* genomes, float* values, size_t stride, void* stream);

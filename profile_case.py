@@ -62,7 +62,15 @@ def main() -> None:
     ap.add_argument("--sampler", default="device", choices=["device", "host"], help="where the samples are drawn")
     ap.add_argument("--line-search", default="", help="step-size factors of a line-search ascent arm, e.g. 0.25,1,4,16")
     ap.add_argument("--cma", type=int, default=0, help="samples an elite a generation of a CMA-ES arm (0: no arm)")
+    ap.add_argument("--cma-kernels", action="store_true",
+                    help="time ce_cma_ask and ce_cma_tell: --creatures emitters, --cma samples an emitter")
+    ap.add_argument("--exploring", action="store_true", help="with --cma-kernels: CMA-ME emitters")
+    ap.add_argument("--audit", action="store_true", help="time ce_audit_device on --creatures synthetic results")
     args = ap.parse_args()
+    if args.cma_kernels:
+        return cma_kernels(args)
+    if args.audit:
+        return audit_case(args)
     if args.generations:
         return generations(args)
     if args.adjoint:
@@ -82,6 +90,114 @@ def main() -> None:
            "creature_substeps": ce.creature_substeps(mine, world),
            "record_bytes": int(wave.lanes.nbytes + wave.muscles.nbytes + wave.heads.nbytes)}
     print(json.dumps(out))
+
+
+def _timed(torch, fn, reps: int) -> float:
+    """Mean milliseconds of fn() over reps runs, CUDA events on the current
+    stream, after two untimed runs."""
+    for _ in range(2):
+        fn()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def cma_kernels(args) -> None:
+    """ce_cma_ask and ce_cma_tell at scale: --creatures emitters of the
+    workload's bodies, --cma (default 16) samples an emitter a generation."""
+    import torch
+
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200.cma import CmaEmitters, dims
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    w = WORKLOADS[args.workload]
+    E, per = args.creatures, args.cma or 16
+    templates = ce.generate(w.spec, E)
+    opt = CmaEmitters(templates, exploring=True if args.exploring else None)
+    n = E * per
+    state = {}
+
+    # Device time of the kernels alone: CmaEmitters brackets each ce_cma_ask
+    # and ce_cma_tell call with CUDA events (kernel_seconds).
+    for _ in range(2):
+        state["genes"], _ = opt.ask_device(n, seed=1, generation=0, first=0)
+    opt.kernel_seconds()
+    for _ in range(5):
+        state["genes"], _ = opt.ask_device(n, seed=1, generation=0, first=0)
+    ask_ms = opt.kernel_seconds() / 5 * 1e3
+    on, ob, om, ost, og = state["genes"]
+    keys = torch.randn(n, device=opt.device)
+    for _ in range(2):
+        opt.tell_device((on, ob, om, og), keys, 0, n)
+    opt.kernel_seconds()
+    for _ in range(5):
+        opt.tell_device((on, ob, om, og), keys, 0, n)
+    tell_ms = opt.kernel_seconds() / 5 * 1e3
+    D = dims(templates.genomes, np.full(E, args.exploring) if args.exploring else None)
+    gene_bytes = sum(int(t.numel()) for t in (on, ob, om, og) + ((ost,) if ost is not None else ()))
+    state_bytes = int(D.sum()) * 4 * 4 + E * 4
+    print(json.dumps({"case": "cma kernels", "workload": args.workload, "emitters": E, "samples": n,
+                      "mode": "cma-me" if args.exploring else "optimizer", "mean_coordinates": float(D.mean()),
+                      "ask_ms": ask_ms, "tell_ms": tell_ms, "samples_per_s": n / (ask_ms * 1e-3),
+                      "ask_genes_bytes": gene_bytes, "ask_write_gbs": gene_bytes / (ask_ms * 1e-3) / 1e9,
+                      "state_bytes": state_bytes,
+                      "tell_bytes": state_bytes * 2 + gene_bytes,
+                      "tell_gbs": (state_bytes * 2 + gene_bytes) / (tell_ms * 1e-3) / 1e9}))
+
+
+def audit_case(args) -> None:
+    """ce_audit_device on --creatures synthetic trials: random trace words,
+    one creature in 128 an audit creature (rungs::AUDIT_ONE_IN), random
+    screen positions and bars."""
+    import ctypes as C
+
+    import torch
+
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200 import api
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    count = args.creatures
+    rng = np.random.default_rng(5)
+    pop = ce.generate(WORKLOADS[args.workload].spec, min(count, 65_536))
+    reps = np.arange(count) % len(pop)
+    genomes = pop.genomes[reps].copy()
+    genomes["flags"] = np.where(rng.random(count) < 1 / 128, 1, 0).astype(np.uint32)
+    words = rng.integers(0, 1 << 32, size=(count, 7), dtype=np.uint64).astype(np.uint32) & np.uint32(0x7bff7bff)
+    words[:, 2] = (words[:, 2] & 0xffff) | (rng.integers(1, 1300, count).astype(np.uint32) << 16)
+    res = np.zeros(count, ce.RESULT_DTYPE)
+    for k, f in enumerate(("contact_hi", "lift_hi", "ground_hi", "previous_center_y", "vertical_extremum",
+                           "vertical_trend", "gait_turns")):
+        res[f] = words[:, k].view(np.float32)
+    res["screen_x"] = rng.normal(2.0, 1.5, count).astype(np.float32)
+    bars = rng.normal(2.0, 0.5, count).astype(np.float32)
+    dev = torch.device("cuda", 0)
+
+    def up(arr):
+        return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(dev)
+
+    dr, dg, dm, db = up(res), up(genomes), up(pop.muscles), up(bars)
+    L = api.lib()
+    scratch = torch.empty(int(L.ce_audit_scratch_bytes(count)), dtype=torch.uint8, device=dev)
+    out = torch.empty(C.sizeof(api.AuditC), dtype=torch.uint8, device=dev)
+    words_out = torch.empty(2 * 65_536 * 6, dtype=torch.int16, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def run():
+        api._check(L.ce_audit_device(dr.data_ptr(), dg.data_ptr(), dm.data_ptr(), db.data_ptr(), count,
+                                     scratch.data_ptr(), scratch.numel(), out.data_ptr(), words_out.data_ptr(),
+                                     65_536, stream.cuda_stream), "ce_audit_device")
+
+    ms = _timed(torch, run, 10)
+    a = api.AuditC.from_buffer_copy(out.cpu().numpy().tobytes())
+    once = count * (ce.RESULT_DTYPE.itemsize + api.GENOME_DTYPE.itemsize + 4)
+    print(json.dumps({"case": "rung audit", "trials": count, "audit_rows": int(a.rows), "ms": ms,
+                      "trials_per_s": count / (ms * 1e-3), "bytes_read_once": once,
+                      "gbs_read_once": once / (ms * 1e-3) / 1e9}))
 
 
 def refined(args) -> None:
