@@ -199,3 +199,29 @@ def test_emitter_moves_toward_its_better_samples(engine, mode):
     before = opt.state(0)[0][0]
     opt.tell(shifted, np.array([4.0, 1.0, 3.0, 2.0], np.float32), first=0)
     assert opt.state(0)[0][0] > before
+
+
+@pytest.mark.parametrize("mode", ["optimizer", "cma-me"])
+def test_tell_breaks_ties_by_sample_index(engine, mode):
+    # Keys rounded to 0.5 tie in runs that straddle the cut at the mu best;
+    # the device sorts ties by sample index, as the restatement does (the
+    # reference's unstable sort leaves their order open).
+    E = 3
+    pop = ce.generate(SPEC, E)
+    ex = modes(mode, E)
+    opt = cma.CmaEmitters(pop, exploring=ex)
+    rng = np.random.default_rng(11)
+    random_state(opt, rng)
+    before = [opt.state(e) for e in range(E)]
+    count = E * 60
+    samples = opt.ask(count, seed=8, first=0, friction=(0.0, 1.0))
+    keys = (np.round(rng.normal(1.0, 1.0, count) * 2.0) / 2.0).astype(np.float32)
+    assert len(np.unique(keys)) < count // 4
+    opt.tell(samples, keys, first=0)
+    for e in range(E):
+        mine = [c for c in range(count) if c % E == e]
+        want = R.tell(before[e], body(pop, e), [body(samples, c) for c in mine], keys[mine], ex[e])
+        have = opt.state(e)
+        np.testing.assert_allclose(have[0], want[0], rtol=1e-5, atol=2e-6)
+        np.testing.assert_allclose(have[1], want[1], rtol=1e-4, atol=1e-5)
+        np.testing.assert_allclose(have[4], want[4], rtol=1e-5)
