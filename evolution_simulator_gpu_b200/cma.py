@@ -46,6 +46,13 @@ def dims(genomes: np.ndarray, exploring=None) -> np.ndarray:
     return np.where(np.asarray(exploring, bool), 4 * n + b + 8 * m, opt)
 
 
+class Genes(tuple):
+    """The device byte tensors of one ask: (nodes, bones, muscles, strength
+    or None, genomes); `rows` holds its node, bone and muscle rows and its
+    sample count."""
+    rows: tuple
+
+
 class CmaEmitters:
     """One CMA-ES emitter per template body, on GPU `device`. `exploring`
     (one flag an emitter, or None) makes an emitter a CMA-ME emitter."""
@@ -134,15 +141,15 @@ class CmaEmitters:
                                     None if vals is None else vals.data_ptr(), stride, self._stream.cuda_stream),
                        "ce_cma_ask")
         self.asked = first + count
-        self._rows = (rn.value, rb.value, rm.value, count)
-        return (on, ob, om, ost, og), (None if vals is None else vals[:count])
+        genes = Genes((on, ob, om, ost, og))
+        genes.rows = (rn.value, rb.value, rm.value, count)
+        return genes, (None if vals is None else vals[:count])
 
     def download(self, genes) -> api.Population:
-        """The genes of the last ask_device (its device tensors) as a host
-        population."""
+        """The genes of an ask_device (its Genes) as a host population."""
         on, ob, om, ost, og = genes
         self._stream.synchronize()
-        rn, rb, rm, count = self._rows
+        rn, rb, rm, count = genes.rows
 
         def back(t, rows, dtype):
             return t.cpu().numpy()[:rows * dtype.itemsize].view(dtype).copy()

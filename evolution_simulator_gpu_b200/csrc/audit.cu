@@ -323,6 +323,7 @@ extern "C" ce_status ce_audit_device(const ce_result* results, const ce_genome* 
         ce::set_error(std::string("ce_audit_device: ") + cudaGetErrorString(e));
         return CE_ERR_DEVICE;
     }
+    if (count == 0) return CE_OK;  // every tally and sum is zero
     uint32_t* tile_rows = static_cast<uint32_t*>(scratch);
     uint32_t* row_index = tile_rows + 4096;
     const unsigned tiles = (unsigned)std::min<size_t>(148u * 8u, std::max<size_t>(1u, (count + kTile - 1u) / kTile));
