@@ -291,6 +291,73 @@ def effects_bench(eng) -> dict:
 
 
 # ---------------------------------------------------------------- engine arm
+def f3_bench(d_results, pop, wave, dev) -> dict:
+    """Row f3 on this generation: the rung audit of its results (population
+    order; audit creatures flagged as rungs::is_audit flags them, bars at the
+    generation's median 5 s position) and a CMA ask and tell of 16,384
+    optimizer emitters x 16 samples on the refine workload's bodies; CUDA
+    events around the library calls, after two untimed calls."""
+    import ctypes as C
+
+    import torch
+
+    import evolution_simulator_gpu_b200 as ce
+    from evolution_simulator_gpu_b200 import api
+    from evolution_simulator_gpu_b200.cma import CmaEmitters
+    from evolution_simulator_gpu_b200.configs import WORKLOADS
+    n = len(wave)
+    inv = torch.from_numpy(np.argsort(wave.slots).astype(np.int64)).to(dev)
+    d_res = d_results.view(n, 19).index_select(0, inv).contiguous()
+    genomes = pop.genomes.copy()
+    genomes["flags"] = api.audit_flags(1, 0, np.arange(n))
+    screen_x = d_res[:, api.RESULT_FIELDS.index("screen_x")].cpu().numpy()
+    bars = np.full(n, np.float32(np.median(screen_x)), np.float32)
+
+    def up(arr):
+        return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(dev)
+
+    d_g, d_m, d_b = up(genomes), up(pop.muscles), up(bars)
+    L = api.lib()
+    scratch = torch.empty(int(L.ce_audit_scratch_bytes(n)), dtype=torch.uint8, device=dev)
+    out = torch.empty(C.sizeof(api.AuditC), dtype=torch.uint8, device=dev)
+    words = torch.empty(2 * 65_536 * 6, dtype=torch.int16, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def audit():
+        api._check(L.ce_audit_device(d_res.data_ptr(), d_g.data_ptr(), d_m.data_ptr(), d_b.data_ptr(), n,
+                                     scratch.data_ptr(), scratch.numel(), out.data_ptr(), words.data_ptr(), 65_536,
+                                     stream.cuda_stream), "ce_audit_device")
+
+    for _ in range(2):
+        audit()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(10):
+        audit()
+    b.record(stream)
+    b.synchronize()
+    audit_ms = a.elapsed_time(b) / 10
+    rows = int(api.AuditC.from_buffer_copy(out.cpu().numpy().tobytes()).rows)
+
+    E, per = 16_384, 16
+    opt = CmaEmitters(ce.generate(WORKLOADS["refine"].spec, E), device=dev.index)
+    for _ in range(2):
+        genes, _ = opt.ask_device(E * per, seed=1, first=0)
+    keys = torch.randn(E * per, device=dev)
+    opt.tell_device(genes[:3] + genes[4:], keys, 0, E * per)
+    opt.kernel_seconds()
+    for _ in range(5):
+        genes, _ = opt.ask_device(E * per, seed=1, first=0)
+    ask_ms = opt.kernel_seconds() / 5 * 1e3
+    for _ in range(5):
+        opt.tell_device(genes[:3] + genes[4:], keys, 0, E * per)
+    tell_ms = opt.kernel_seconds() / 5 * 1e3
+    return {"audit": {"trials": n, "audit_rows": rows, "ms": audit_ms, "trials_per_s": n / (audit_ms * 1e-3)},
+            "cma": {"emitters": E, "samples": E * per, "ask_ms": ask_ms, "tell_ms": tell_ms,
+                    "samples_per_s": E * per / (ask_ms * 1e-3)},
+            "timing": "CUDA events around the library calls (ce_audit_device; ce_cma_ask, ce_cma_tell)"}
+
+
 def run_engine(args):
     world_size, rank, local = dist_setup(args.gpus)
     import torch
@@ -381,6 +448,7 @@ def run_engine(args):
         cpu = cpu_baseline(wave, world, args.cpu_seconds)
         adjoint = adjoint_bench(eng) if not args.no_adjoint else None
         effects = effects_bench(eng) if not args.no_effects else None
+        f3 = f3_bench(d_results, pop, wave, dev)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -400,6 +468,7 @@ def run_engine(args):
                                        "results for the same generation in the same packed order"},
             "gpu_launches": (BUCKET_KERNELS + 1) * args.steps, "gpu_launches_e2e": e2e_launches,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "adjoint": adjoint, "effects": effects,
+            "f3": f3,
         }
         print(json.dumps(line), flush=True)
     eng.close()

@@ -991,6 +991,20 @@ def shape_classes(pop: Population, wave: "WavePack", indices=None, global_layout
     return out
 
 
+def audit_flags(seed: int, round_: int, slots) -> np.ndarray:
+    """rungs::is_audit (src/rungs.rs:153-168) for each ring slot of breeding
+    round `round_`: rungs::AUDIT (1) on one slot in 128, picked by a hash of
+    (seed, round, slot), else 0."""
+    s = np.asarray(slots, np.uint64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) ^ (np.uint64(round_) * np.uint64(0x9e3779b97f4a7c15)) ^ (s * np.uint64(0xd1342543de82ef95))
+        x = x + np.uint64(0x9e3779b97f4a7c15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+        x = x ^ (x >> np.uint64(31))
+    return (x % np.uint64(128) == 0).astype(np.uint32)
+
+
 def audit(results: np.ndarray, pop: "Population", bars: np.ndarray, a_cap: int = 1 << 16, device=None) -> dict:
     """The rung audit of a batch on the GPU (ce_audit_device): `results` in
     population order, `pop` the batch's genomes (flags, first muscle's

@@ -80,3 +80,27 @@ def test_note_counts_trials_steps_and_stops():
              trace_words(1, 1, 1, 300, code=0), trace_words(1, 1, 1, 1200, code=1 << 6)]
     res = results_of(words, screened=[1.0, 2.5, 5.0, 0.0])
     assert A.note(res) == (4, 60 + 150 + 300 + 1200, [1, 1, 1])
+
+
+def test_one_in_128_slots_are_audit_creatures():
+    # one_in_128_slots_are_audit_creatures (src/rungs/tests.rs:56-70).
+    n = 2_000_000
+    share = ce.api.audit_flags(5051, 7, np.arange(n)).mean()
+    assert abs(share - 1 / 128) < 5e-4
+    a = ce.api.audit_flags(1, 2, np.arange(4096))
+    assert (a == ce.api.audit_flags(1, 2, np.arange(4096))).all()
+    assert (a != ce.api.audit_flags(1, 3, np.arange(4096))).any()
+
+
+def test_audit_flags_follow_the_hash():
+    # is_audit's hash (src/rungs.rs:157-168) for one slot, in Python integers.
+    def is_audit(seed, round_, slot):
+        m = (1 << 64) - 1
+        x = seed ^ (round_ * 0x9e3779b97f4a7c15 & m) ^ (slot * 0xd1342543de82ef95 & m)
+        x = (x + 0x9e3779b97f4a7c15) & m
+        x = ((x ^ (x >> 30)) * 0xbf58476d1ce4e5b9) & m
+        x = ((x ^ (x >> 27)) * 0x94d049bb133111eb) & m
+        return (x ^ (x >> 31)) % 128 == 0
+    slots = np.arange(50_000)
+    want = np.array([is_audit(77, 5, int(k)) for k in slots])
+    assert (ce.api.audit_flags(77, 5, slots).astype(bool) == want).all() and want.sum() > 300
