@@ -225,3 +225,37 @@ def test_tell_breaks_ties_by_sample_index(engine, mode):
         np.testing.assert_allclose(have[0], want[0], rtol=1e-5, atol=2e-6)
         np.testing.assert_allclose(have[1], want[1], rtol=1e-4, atol=1e-5)
         np.testing.assert_allclose(have[4], want[4], rtol=1e-5)
+
+
+@pytest.mark.parametrize("mode", ["optimizer", "cma-me"])
+def test_bodies_at_the_engines_limits(engine, mode):
+    # 32 nodes and 96 muscles: 1,052 optimizer coordinates (927 CMA-ME), the
+    # size of the tell kernel's shared coordinate arrays.
+    spec = ce.GenSpecPy(seed=9, min_nodes=32, max_nodes=32, min_muscles=96, max_muscles=96, muscle_rule=1)
+    E = 2
+    pop = ce.generate(spec, E)
+    ex = modes(mode, E)
+    opt = cma.CmaEmitters(pop, exploring=ex)
+    rng = np.random.default_rng(21)
+    random_state(opt, rng)
+    before = [opt.state(e) for e in range(E)]
+    assert len(before[0][0]) == (927 if ex[0] else 1052)
+    count = E * 24
+    genes, vals = opt.ask_device(count, seed=2, first=0, values=True, friction=(0.0, 1.0))
+    vals = vals.cpu().numpy()
+    samples = opt.download(genes)
+    for c in range(count):
+        e = c % E
+        want_v = R.sample(before[e], body(pop, e), ex[e], c, seed=2)
+        assert (vals[c, :len(want_v)] == want_v).all()
+    keys = rng.normal(1.0, 1.0, count).astype(np.float32)
+    opt.tell(samples, keys, first=0)
+    for e in range(E):
+        mine = list(range(e, count, E))
+        want = R.tell(before[e], body(pop, e), [body(samples, c) for c in mine], keys[mine], ex[e])
+        have = opt.state(e)
+        np.testing.assert_allclose(have[0], want[0], rtol=1e-5, atol=2e-6)
+        np.testing.assert_allclose(have[1], want[1], rtol=1e-4, atol=1e-5)
+        np.testing.assert_allclose(have[2], want[2], rtol=1e-4, atol=1e-4)
+        np.testing.assert_allclose(have[3], want[3], rtol=1e-4, atol=1e-4)
+        np.testing.assert_allclose(have[4], want[4], rtol=1e-5)
