@@ -80,3 +80,27 @@ def test_audit_of_an_empty_batch(engine):
     got = api.audit(res, api.Population(pop.nodes, pop.bones, pop.muscles, pop.genomes[:0], pop.strength),
                     np.zeros(0, np.float32))
     assert got["creatures"] == 0 and got["rows"] == 0 and got["sums"][0][0][0] == 0
+
+
+def test_audit_words_stop_at_the_callers_capacity(engine):
+    # Class A's feature words go to the first a_cap rows only (here fewer
+    # than one chunk of 256 rows holds, and more than one); the sums count
+    # every row.
+    rng = np.random.default_rng(4)
+    count = 20_000
+    pop = ce.generate(WORKLOADS["game"].spec, count)
+    words = rng.integers(0, 1 << 32, size=(count, 7), dtype=np.uint64).astype(np.uint32) & np.uint32(0x7bff7bff)
+    words[:, 2] = (words[:, 2] & 0xffff) | (rng.integers(200, 1300, count).astype(np.uint32) << 16)
+    res = np.zeros(count, ce.RESULT_DTYPE)
+    for k, f in enumerate(A.TRACE_FIELDS):
+        res[f] = words[:, k].view(np.float32)
+    res["screen_x"] = rng.normal(2.0, 1.0, count).astype(np.float32)
+    pop.genomes["flags"] = np.where(rng.random(count) < 0.1, A.AUDIT, 0).astype(np.uint32)
+    bars = np.full(count, 1.5, np.float32)
+    _, sums, a_rows = A.gen_audit(res, pop.genomes["flags"], periods_of(pop), bars)
+    assert len(a_rows[0]) > 600
+    for cap in (37, 300):
+        got = api.audit(res, pop, bars, a_cap=cap)
+        for r in range(2):
+            assert got["sums"][r][0][0] == sums[r][0][0]
+            assert (got["a_words"][r] == a_rows[r][:cap]).all() and len(got["a_words"][r]) == cap
