@@ -232,6 +232,7 @@ def _bind(lib: C.CDLL) -> None:
         "ce_cma_ask": (C.c_int, [P(CmaC), P(CmaDraw), C.c_uint64, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
         "ce_cma_tell": (C.c_int, [P(CmaC), P(PopulationC), C.c_void_p, C.c_uint64, C.c_size_t, C.c_void_p]),
+        "ce_cma_recenter": (C.c_int, [P(CmaC), P(PopulationC), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
         "ce_audit_scratch_bytes": (C.c_size_t, [C.c_size_t]),
         "ce_audit_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
@@ -280,7 +281,7 @@ EXPORTED = ["ce_world_flags", "ce_make_params", "ce_pack_size", "ce_pack", "ce_f
             "ce_tape_seconds", "ce_backward", "ce_backward_checked", "ce_tape_free", "ce_tangent", "ce_gene_gradients", "ce_tape_checkpoints",
             "ce_replay_decode", "ce_sample_rows", "ce_sample_device", "ce_dump_rows", "ce_dump_rows_device", "ce_metrics_device", "ce_shape_classes", "ce_height_bin_edges", "ce_graph_open",
             "ce_graph_launch", "ce_graph_results", "ce_graph_close", "ce_autotune", "ce_cma_offsets", "ce_cma_init",
-            "ce_cma_ask", "ce_cma_tell", "ce_audit_scratch_bytes", "ce_audit_device"]
+            "ce_cma_ask", "ce_cma_tell", "ce_cma_recenter", "ce_audit_scratch_bytes", "ce_audit_device"]
 
 
 def _check(status: int, what: str) -> None:

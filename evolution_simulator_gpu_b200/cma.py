@@ -206,6 +206,53 @@ class CmaEmitters:
             api._check(api.lib().ce_cma_tell(C.byref(self._c), C.byref(pc), keys.data_ptr(), first, count,
                                              self._stream.cuda_stream), "ce_cma_tell")
 
+    def recenter(self, which, bodies: api.Population) -> np.ndarray:
+        """CmaEmitter::recentered (src/qd.rs:2166-2177): emitter which[i]
+        restarts from body i of `bodies` (its template replaced, the mean at
+        the body's coordinates), keeping its covariance, paths and step size
+        when the body's plan is the template's. Bodies whose counts differ
+        from the template's are rejected (True in the returned mask) and
+        leave their emitter as it was."""
+        from .refine import take
+        torch = self._torch
+        which = np.ascontiguousarray(which, np.uint32)
+        if len(np.unique(which)) != len(which):
+            raise ValueError("recenter: the emitters must be distinct")
+        b = take(bodies, np.arange(len(bodies)))
+
+        def up(arr):
+            return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(self.device)
+
+        dn, db, dm, dg, dw = up(b.nodes), up(b.bones), up(b.muscles), up(b.genomes), up(which)
+        ds = None if b.strength is None else up(b.strength)
+        rej = torch.zeros(max(len(which), 1), dtype=torch.int32, device=self.device)
+        pc = api.PopulationC(dn.data_ptr(), db.data_ptr(), dm.data_ptr(), dg.data_ptr(), len(b),
+                             None if ds is None else ds.data_ptr())
+        api._check(api.lib().ce_cma_recenter(C.byref(self._c), C.byref(pc), dw.data_ptr(), len(which),
+                                             rej.data_ptr(), self._stream.cuda_stream), "ce_cma_recenter")
+        rejected = rej.cpu().numpy()[:len(which)].astype(bool)
+        # The host copy of the templates follows the device's.
+        t = self.templates
+        for i, e in enumerate(which):
+            if rejected[i]:
+                continue
+            g, h = t.genomes[e], b.genomes[i]
+            for arr, src, f in ((t.nodes, b.nodes, "node"), (t.bones, b.bones, "bone"), (t.muscles, b.muscles, "muscle")):
+                a0, n = int(g[f + "_start"]), int(g[f + "_count"])
+                arr[a0:a0 + n] = src[int(h[f + "_start"]):int(h[f + "_start"]) + n]
+            if t.strength is not None and b.strength is not None:
+                a0, n = int(g["muscle_start"]), int(g["muscle_count"])
+                t.strength[a0:a0 + n] = b.strength[int(h["muscle_start"]):int(h["muscle_start"]) + n]
+        return rejected
+
+    def converged(self) -> np.ndarray:
+        """CmaEmitter::converged (src/qd.rs:2184-2187): optimizers whose step
+        size has fallen below 0.05."""
+        self._stream.synchronize()
+        sig = self.sigma.cpu().numpy()
+        opt = np.ones(len(self), bool) if self.exploring is None else ~self.exploring.astype(bool)
+        return opt & (sig < 0.05)
+
     def state(self, e: int):
         """Emitter e's (mean, covariance, path_c, path_sigma, sigma) on the
         host."""

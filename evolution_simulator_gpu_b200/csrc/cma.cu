@@ -593,6 +593,47 @@ __global__ void __launch_bounds__(kTellBlock) cma_tell_kernel(const Emitters em,
     }
 }
 
+// CmaEmitter::recentered (src/qd.rs:2166-2177), one thread a pair:
+// emitter which[i] restarts from body i of `b`. Counts that differ from the
+// template's leave the emitter as it was (rejected[i] = 1). Otherwise the
+// plan test runs on the old template, the body's genes replace the
+// template's, the mean moves to the body's coordinates and the covariance,
+// paths and step size stay when the plan is the template's, else restart as
+// the mode's constructor sets them.
+__global__ void cma_recenter_kernel(const Emitters em, const ce_population b, const uint32_t* which, size_t n,
+                                    uint32_t* rejected) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t e = which[i];
+        const ce_genome tg = em.t.genomes[e], bg = b.genomes[i];
+        const bool fits = e < em.t.count && bg.node_count == tg.node_count && bg.bone_count == tg.bone_count &&
+                          bg.muscle_count == tg.muscle_count;
+        if (rejected) rejected[i] = fits ? 0u : 1u;
+        if (!fits) continue;
+        const bool keep = same_plan(em.t, tg, b, bg);
+        ce_node_gene* tn = const_cast<ce_node_gene*>(em.t.nodes) + tg.node_start;
+        ce_bone_gene* tb = const_cast<ce_bone_gene*>(em.t.bones) + tg.bone_start;
+        ce_muscle_gene* tm = const_cast<ce_muscle_gene*>(em.t.muscles) + tg.muscle_start;
+        for (unsigned k = 0u; k < tg.node_count; k++) tn[k] = b.nodes[bg.node_start + k];
+        for (unsigned k = 0u; k < tg.bone_count; k++) tb[k] = b.bones[bg.bone_start + k];
+        for (unsigned k = 0u; k < tg.muscle_count; k++) tm[k] = b.muscles[bg.muscle_start + k];
+        if (em.t.strength_scale && b.strength_scale) {
+            float* ts = const_cast<float*>(em.t.strength_scale) + tg.muscle_start;
+            for (unsigned k = 0u; k < tg.muscle_count; k++) ts[k] = b.strength_scale[bg.muscle_start + k];
+        }
+        const Layout l = Layout::of(tg, em.t.bones, em.explores(e));
+        const uint64_t off = em.offsets[e];
+        for (unsigned d = 0u; d < l.dims(); d++) {
+            em.mean[off + d] = parameter(l, tn, tb, tm, d);
+            if (!keep) {
+                em.covariance[off + d] = 1.0f;
+                em.path_c[off + d] = 0.0f;
+                em.path_sigma[off + d] = 0.0f;
+            }
+        }
+        if (!keep) em.sigma[e] = l.exploring ? 0.12f : 0.5f;
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -729,4 +770,17 @@ extern "C" ce_status ce_cma_tell(const ce_cma* cma, const ce_population* samples
     cma_tell_kernel<<<(unsigned)E, kTellBlock, 0, static_cast<cudaStream_t>(stream)>>>(emitters_of(cma), *samples,
                                                                                          keys, first, count);
     return launched("ce_cma_tell");
+}
+
+extern "C" ce_status ce_cma_recenter(const ce_cma* cma, const ce_population* bodies, const uint32_t* which, size_t n,
+                                     uint32_t* rejected, void* stream) {
+    if (!usable(cma) || !bodies || (n && (!which || !bodies->genomes || !bodies->nodes || !bodies->bones ||
+                                          !bodies->muscles))) {
+        ce::set_error("ce_cma_recenter: null argument or no emitters");
+        return CE_ERR_INVALID;
+    }
+    if (n == 0) return CE_OK;
+    cma_recenter_kernel<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(emitters_of(cma), *bodies, which,
+                                                                                     n, rejected);
+    return launched("ce_cma_recenter");
 }

@@ -430,6 +430,16 @@ ce_status ce_cma_ask(const ce_cma* cma, const ce_cma_draw* draw, uint64_t first,
  * paths, covariance and step size. At most 4096 samples an emitter a call. */
 ce_status ce_cma_tell(const ce_cma* cma, const ce_population* samples, const float* keys, uint64_t first,
                       size_t count, void* stream);
+/* CmaEmitter::recentered (src/qd.rs:2166-2177) for emitters which[0..n)
+ * (device array, distinct emitters): emitter which[i] restarts from body i of `bodies`, which
+ * must have its template's node, bone and muscle counts (else it is left as
+ * it was and rejected[i], a device array or NULL, is set to 1). The body's
+ * genes overwrite the template's (the templates' memory must be writable),
+ * the mean moves to the body's coordinates, and the covariance, paths and
+ * step size are kept when the body's plan (bone and muscle connections) is
+ * the template's, else restart as the mode's constructor sets them. */
+ce_status ce_cma_recenter(const ce_cma* cma, const ce_population* bodies, const uint32_t* which, size_t n,
+                          uint32_t* rejected, void* stream);
 
 /* ---- rung audit on the device ---- */
 /* Sums::add's sums of one class of feature vectors (src/rungs.rs:286-299):

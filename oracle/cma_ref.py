@@ -17,6 +17,8 @@ of the device's ce_cma_init / ce_cma_ask / ce_cma_tell. Only tests/ use it.
   2381-2402) for the child of ring slot g.
 * ``tell``: tell with tell_optimizing or tell_exploring (src/qd.rs:
   2213-2243, 2290-2376, 2405-2474), with ties in key broken by sample index.
+* ``recentered``: CmaEmitter::recentered (src/qd.rs:2166-2177), for either
+  mode.
 
 Every operation is float32, in the reference's order; ln and exp are numpy's.
 """
@@ -408,3 +410,17 @@ def tell(state, template, samples, fitness, exploring=False):
     if pairs[L // 2][0] < f32(f32(0.25) * pairs[0][0]):
         sigma = max(f32(sigma * f32(0.6)), f32(0.01))
     return mean, cov, pc, ps, sigma
+
+
+def recentered(state, template, body, exploring=False):
+    """The state an emitter restarts in from `body`: the mean at the body's
+    coordinates; covariance, paths and step size kept when the body's plan
+    is the template's, else the mode's constructor's (unit covariance, zero
+    paths, 0.5 or 0.12)."""
+    mean = explore_parameters(*body) if exploring else parameters(*body)
+    if same_plan(template, body) and len(mean) == len(state[0]):
+        return mean, np.array(state[1], np.float32), np.array(state[2], np.float32), \
+            np.array(state[3], np.float32), f32(state[4])
+    D = len(mean)
+    return mean, np.ones(D, np.float32), np.zeros(D, np.float32), np.zeros(D, np.float32), \
+        f32(0.12 if exploring else 0.5)

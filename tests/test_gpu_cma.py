@@ -259,3 +259,47 @@ def test_bodies_at_the_engines_limits(engine, mode):
         np.testing.assert_allclose(have[2], want[2], rtol=1e-4, atol=1e-4)
         np.testing.assert_allclose(have[3], want[3], rtol=1e-4, atol=1e-4)
         np.testing.assert_allclose(have[4], want[4], rtol=1e-5)
+
+
+@pytest.mark.parametrize("mode", ["optimizer", "cma-me"])
+def test_recentered_keeps_the_learned_steps_for_the_same_plan(engine, mode):
+    # CmaEmitter::recentered (src/qd.rs:2166-2177): emitter 0 restarts from a
+    # body of its own plan (keeps covariance, paths and step size), emitter 1
+    # from a body whose first muscle joins other bones (restarts), emitter 2
+    # from a body of other counts (rejected: left as it was).
+    E = 3
+    pop = ce.generate(SPEC, E)
+    ex = modes(mode, E)
+    opt = cma.CmaEmitters(pop, exploring=ex)
+    random_state(opt, np.random.default_rng(31))
+    before = [opt.state(e) for e in range(E)]
+    samples = opt.ask(E, seed=5, first=0, friction=(0.0, 1.0))
+    other = ce.generate(ce.GenSpecPy(seed=77, min_nodes=3, max_nodes=10, max_muscles=20), 50)
+    k = int(np.flatnonzero(other.genomes["node_count"] != pop.genomes["node_count"][2])[0])
+    bodies = refine.concat([refine.take(samples, np.array([0, 1])), refine.take(other, np.array([k]))])
+    m1 = int(bodies.genomes["muscle_start"][1])
+    bodies.muscles["bone_b"][m1] = (bodies.muscles["bone_b"][m1] + 1) % bodies.genomes["bone_count"][1]
+    rejected = opt.recenter([0, 1, 2], bodies)
+    assert list(rejected) == [False, False, True]
+    for e in range(2):
+        want = R.recentered(before[e], body(pop, e), body(bodies, e), ex[e])
+        have = opt.state(e)
+        if ex[e]:
+            assert (have[0] == want[0]).all()
+        else:
+            np.testing.assert_allclose(have[0], want[0], rtol=4e-7, atol=4e-7)
+        for x, y in zip(have[1:], want[1:]):
+            assert (np.asarray(x) == np.asarray(y)).all()
+    assert (opt.state(0)[1] == before[0][1]).all() and opt.state(0)[4] == before[0][4]
+    assert (opt.state(1)[1] == 1).all() and opt.state(1)[4] == np.float32(0.12 if ex[1] else 0.5)
+    for x, y in zip(opt.state(2), before[2]):
+        assert (np.asarray(x) == np.asarray(y)).all()
+    # The device templates follow: the next ask samples around the new bodies.
+    t = opt.templates
+    assert (opt._t[0].cpu().numpy().view(t.nodes.dtype) == t.nodes).all()
+    assert (opt._t[2].cpu().numpy().view(t.muscles.dtype) == t.muscles).all()
+    assert (t.nodes[:int(t.genomes["node_count"][0])] == body(bodies, 0)[0]).all()
+    # converged (src/qd.rs:2184-2187): an optimizer below a step size of 0.05.
+    s0 = opt.state(0)
+    opt.set_state(0, *s0[:4], 0.04)
+    assert opt.converged()[0] == (not ex[0]) and not opt.converged()[1]
