@@ -198,3 +198,35 @@ def test_dims_match_the_parameter_vectors():
     for i in range(len(pop)):
         assert d[i] == len(R.parameters(*body(pop, i)))
     assert refine.take(pop, np.arange(3)).genomes["node_start"][0] == 0
+
+
+def test_device_entry_points_check_their_arguments_without_a_gpu():
+    # Each check returns before any CUDA call, so fake (never dereferenced)
+    # device addresses stand in for real ones.
+    L = ce.lib()
+    fake = 4096
+    pc = api.PopulationC(fake, fake, fake, fake, 4, None)
+    c = api.CmaC(pc, None, fake, fake, fake, fake, fake, fake)
+    # More than 4096 samples an emitter in one tell.
+    assert L.ce_cma_tell(C.byref(c), C.byref(pc), fake, 0, 4 * 4096 + 1, None) == ce.CE_ERR_INVALID
+    assert b"4096" in L.ce_last_error()
+    # An empty diameter or friction range.
+    bad = cma.CmaEmitters.draw(size=(0.12, 0.06))
+    assert L.ce_cma_ask(C.byref(c), C.byref(bad), 0, 8, fake, fake, fake, None, fake, None, 0, None) \
+        == ce.CE_ERR_INVALID
+    bad = cma.CmaEmitters.draw(friction=(1.0, 0.5))
+    assert L.ce_cma_ask(C.byref(c), C.byref(bad), 0, 8, fake, fake, fake, None, fake, None, 0, None) \
+        == ce.CE_ERR_INVALID
+    # Values asked for with no stride.
+    ok = cma.CmaEmitters.draw()
+    assert L.ce_cma_ask(C.byref(c), C.byref(ok), 0, 8, fake, fake, fake, None, fake, fake, 0, None) \
+        == ce.CE_ERR_INVALID
+    # Recentering needs its bodies and emitter list.
+    assert L.ce_cma_recenter(C.byref(c), None, fake, 1, None, None) == ce.CE_ERR_INVALID
+    assert L.ce_cma_recenter(C.byref(c), C.byref(pc), None, 1, None, None) == ce.CE_ERR_INVALID
+    # The audit's scratch must hold ce_audit_scratch_bytes(count).
+    need = L.ce_audit_scratch_bytes(1000)
+    assert need >= 1000 * 4
+    assert L.ce_audit_device(fake, fake, fake, fake, 1000, fake, need - 1, fake, None, 0, None) == ce.CE_ERR_INVALID
+    assert b"scratch" in L.ce_last_error()
+    assert L.ce_audit_device(None, fake, fake, fake, 1000, fake, need, fake, None, 0, None) == ce.CE_ERR_INVALID
