@@ -253,6 +253,34 @@ class CmaEmitters:
         opt = np.ones(len(self), bool) if self.exploring is None else ~self.exploring.astype(bool)
         return opt & (sig < 0.05)
 
+    def save(self, path) -> None:
+        """The emitters as one .npz file: templates, modes, every emitter's
+        mean, covariance, paths and step size, and where the next ask
+        starts (the reference keeps its emitters in its search-state saves,
+        tests/search_state.rs:769)."""
+        self._stream.synchronize()
+        t = self.templates
+        extra = {} if t.strength is None else {"strength": t.strength}
+        if self.exploring is not None:
+            extra["exploring"] = self.exploring
+        np.savez(path, nodes=t.nodes, bones=t.bones, muscles=t.muscles, genomes=t.genomes,
+                 mean=self.mean.cpu().numpy(), covariance=self.covariance.cpu().numpy(),
+                 path_c=self.path_c.cpu().numpy(), path_sigma=self.path_sigma.cpu().numpy(),
+                 sigma=self.sigma.cpu().numpy(), asked=np.uint64(self.asked), **extra)
+
+    @classmethod
+    def load(cls, path, device=None, stream=None) -> "CmaEmitters":
+        """Emitters as `save` left them, on GPU `device`."""
+        d = np.load(path)
+        t = api.Population(d["nodes"], d["bones"], d["muscles"], d["genomes"],
+                           d["strength"] if "strength" in d else None)
+        out = cls(t, exploring=d["exploring"] if "exploring" in d else None, device=device, stream=stream)
+        torch = out._torch
+        for name in ("mean", "covariance", "path_c", "path_sigma", "sigma"):
+            getattr(out, name).copy_(torch.from_numpy(d[name]).to(out.device))
+        out.asked = int(d["asked"])
+        return out
+
     def state(self, e: int):
         """Emitter e's (mean, covariance, path_c, path_sigma, sigma) on the
         host."""

@@ -303,3 +303,25 @@ def test_recentered_keeps_the_learned_steps_for_the_same_plan(engine, mode):
     s0 = opt.state(0)
     opt.set_state(0, *s0[:4], 0.04)
     assert opt.converged()[0] == (not ex[0]) and not opt.converged()[1]
+
+
+def test_saved_emitters_resume_where_they_stopped(engine, tmp_path):
+    # A save and a load between two generations: the resumed emitters hold
+    # the same state and draw the same next samples, to the bit.
+    E = 5
+    pop = ce.generate(SPEC, E)
+    opt = cma.CmaEmitters(pop, exploring=modes("mixed", E))
+    rng = np.random.default_rng(41)
+    for gen in range(2):
+        kids = opt.ask(E * 12, seed=3, generation=gen, friction=(0.0, 1.0))
+        opt.tell(kids, rng.normal(1.0, 1.0, len(kids)).astype(np.float32))
+    opt.save(tmp_path / "emitters.npz")
+    back = cma.CmaEmitters.load(tmp_path / "emitters.npz")
+    assert back.asked == opt.asked
+    for e in range(E):
+        for x, y in zip(back.state(e), opt.state(e)):
+            assert (np.asarray(x) == np.asarray(y)).all()
+    a = opt.ask(E * 12, seed=3, generation=2, friction=(0.0, 1.0))
+    b = back.ask(E * 12, seed=3, generation=2, friction=(0.0, 1.0))
+    for f in ("nodes", "bones", "muscles", "genomes", "strength"):
+        assert (getattr(a, f).view(np.uint8) == getattr(b, f).view(np.uint8)).all()
