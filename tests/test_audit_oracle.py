@@ -104,3 +104,43 @@ def test_audit_flags_follow_the_hash():
     slots = np.arange(50_000)
     want = np.array([is_audit(77, 5, int(k)) for k in slots])
     assert (ce.api.audit_flags(77, 5, slots).astype(bool) == want).all() and want.sum() > 300
+
+
+def test_a_second_restatement_agrees():
+    # GenAudit::of written again, vectorised: the same rows, classes, counts
+    # and class A words exactly; the float64 sums within rounding of the
+    # summation order (np.sum pairs its terms).
+    rng = np.random.default_rng(8)
+    n = 20_000
+    words = rng.integers(0, 1 << 32, size=(n, 7), dtype=np.uint64).astype(np.uint32)
+    finite = rng.random((n, 7)) < 0.97
+    words[finite] &= np.uint32(0x7bff7bff)
+    words[:, 2] = (words[:, 2] & 0xffff) | (rng.integers(0, 1300, n).astype(np.uint32) << 16)
+    res = results_of(words.tolist(), rng.normal(2.0, 1.5, n).astype(np.float32))
+    flags = (np.where(rng.random(n) < 0.3, A.AUDIT, 0) | np.where(rng.random(n) < 0.1, A.EXEMPT, 0)).astype(np.uint32)
+    periods = rng.uniform(0.2, 3.0, n).astype(np.float32)
+    bars = rng.normal(2.0, 0.5, n).astype(np.float32)
+    bars[rng.random(n) < 0.05] = np.nan
+    rows, sums, a_rows = A.gen_audit(res, flags, periods, bars)
+
+    def halves(w):
+        return (w & 0xffff).astype(np.uint16).view(np.float16).astype(np.float64), \
+            (w >> 16).astype(np.uint16).view(np.float16).astype(np.float64)
+
+    steps = words[:, 2] >> 16
+    is_row = ((flags & A.AUDIT) != 0) & (steps != 0)
+    assert rows == int(is_row.sum())
+    counted = is_row & ((flags & A.EXEMPT) == 0) & np.isfinite(bars)
+    with np.errstate(invalid="ignore"):
+        pass3 = res["screen_x"] >= bars
+    lo, hi = zip(*[halves(words[:, k]) for k in range(7)])
+    ph = periods.astype(np.float16).astype(np.float64)
+    for r in range(2):
+        f = np.stack([hi[0] if r else lo[0], hi[3] if r else lo[3], lo[4 + r], hi[6] if r else lo[6], hi[4 + r], ph], 1)
+        ok = counted & (steps > (150 if r else 60)) & np.isfinite(f).all(1)
+        for k, cls in enumerate((ok & pass3, ok & ~pass3)):
+            x = f[cls]
+            assert sums[r][k][0] == len(x)
+            np.testing.assert_allclose(sums[r][k][1], x.sum(0), rtol=1e-12)
+            np.testing.assert_allclose(np.array(sums[r][k][2]), x.T @ x, rtol=1e-12)
+        assert (a_rows[r] == f[ok & pass3].astype(np.float16).view(np.uint16)).all()

@@ -230,3 +230,43 @@ def test_device_entry_points_check_their_arguments_without_a_gpu():
     assert L.ce_audit_device(fake, fake, fake, fake, 1000, fake, need - 1, fake, None, 0, None) == ce.CE_ERR_INVALID
     assert b"scratch" in L.ce_last_error()
     assert L.ce_audit_device(None, fake, fake, fake, 1000, fake, need, fake, None, 0, None) == ce.CE_ERR_INVALID
+
+
+def test_a_second_restatement_of_the_streams_agrees():
+    # The breeding streams again, vectorised in numpy's wrapping uint64:
+    # stream keys, the genes sub-stream and its Gaussians, for 2,000 slots x
+    # 64 genes, equal to the restatement's integers and floats.
+    u = np.uint64
+
+    def fin(z):
+        z = (z ^ (z >> u(30))) * u(0xbf58476d1ce4e5b9)
+        z = (z ^ (z >> u(27))) * u(0x94d049bb133111eb)
+        return z ^ (z >> u(31))
+
+    def key_of(seed, gen, rnd, slots):
+        with np.errstate(over="ignore"):
+            k = fin(np.full(len(slots), u(seed), u) + u(0x632be59bd9b4e019))
+            for w in (np.full(len(slots), u(gen), u), np.full(len(slots), u(rnd), u), slots.astype(u)):
+                k = fin(k ^ (w * u(0xd1342543de82ef95)))
+        return k
+
+    def keyed_v(key, gene, draw):
+        with np.errstate(over="ignore"):
+            return fin(key + ((u(gene) << u(32)) | u(draw)) * u(0x9e3779b97f4a7c15))
+
+    slots = np.arange(2000, dtype=np.int64)
+    keys = key_of(7, 3, 2, slots)
+    for g in (0, 999, 1999):
+        assert int(keys[g]) == R.stream_key(7, 3, 2, g)
+    genes = keyed_v(keys, 0xffffffff, 0)
+    total = np.zeros((2000, 64), np.int64)
+    for d in range(64):
+        for k in range(3):
+            w = keyed_v(genes, d, k)
+            total[:, d] += ((w & u(0xffff)) + ((w >> u(16)) & u(0xffff)) + ((w >> u(32)) & u(0xffff)) +
+                            (w >> u(48))).astype(np.int64)
+    gauss = (total - 6 * 65535).astype(np.float32) * (np.float32(1.0) / np.float32(65535.0))
+    for g in (0, 1, 500, 1999):
+        want = [R.gene_gaussian(R.keyed(R.stream_key(7, 3, 2, g), R.CURSOR, 0), d) for d in range(64)]
+        assert (gauss[g] == np.array(want, np.float32)).all()
+    assert abs(gauss.mean()) < 0.01 and abs(gauss.std() - 1.0) < 0.01
