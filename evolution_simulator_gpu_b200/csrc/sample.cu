@@ -183,6 +183,11 @@ extern "C" ce_status ce_sample_rows(const ce_genome* parent_genomes, size_t pare
     *nodes = (size_t)(offset(first + count, 0) - offset(first, 0));
     *bones = (size_t)(offset(first + count, 1) - offset(first, 1));
     *muscles = (size_t)(offset(first + count, 2) - offset(first, 2));
+    // A sample's gene starts are 32-bit, counted from the call's first row.
+    if (*nodes > 0xffffffffull || *bones > 0xffffffffull || *muscles > 0xffffffffull || count > 0xffffffffull) {
+        ce::set_error("ce_sample_rows: more than 2^32 - 1 gene rows of a kind in one call; draw fewer samples a call");
+        return CE_ERR_INVALID;
+    }
     return CE_OK;
 }
 

@@ -328,7 +328,8 @@ ce_status ce_dump_rows_device(const ce_result* results, const uint32_t* heads, c
  * deviates come from a counter-based hash of (seed, g, gene, field), so a
  * sample does not depend on the range a call draws. No counterpart in the
  * reference, which samples on the host. ce_sample_rows gives the rows of
- * samples [first, first + count) from the parents' (host) genomes;
+ * samples [first, first + count) from the parents' (host) genomes (at most
+ * 2^32 - 1 rows of a kind a call: the samples' gene starts are 32-bit);
  * ce_sample_device writes them (device pointers; the parents' genes packed
  * in order from row 0; `strength` may be NULL), asynchronous on `stream`
  * after a small synchronous read of the parents' genomes. */

@@ -144,3 +144,15 @@ def test_sample_rows_count_the_tiled_parents():
         assert ce.lib().ce_sample_rows(ce.api._ptr(g), len(parents), first, count, *[C.byref(r) for r in rows]) == 0
         want = [int(g[f][idx].sum()) for f in ("node_count", "bone_count", "muscle_count")]
         assert [r.value for r in rows] == want
+
+
+def test_sample_rows_refuse_more_rows_than_32_bit_starts_hold():
+    import ctypes as C
+    parents = ce.generate(ce.GenSpecPy(seed=2, min_nodes=32, max_nodes=32, min_muscles=96, max_muscles=96,
+                                       muscle_rule=1), 1)
+    rows = [C.c_size_t() for _ in range(3)]
+    g = parents.genomes
+    assert ce.lib().ce_sample_rows(ce.api._ptr(g), 1, 0, 40_000_000, *[C.byref(r) for r in rows]) == 0
+    assert ce.lib().ce_sample_rows(ce.api._ptr(g), 1, 0, 50_000_000, *[C.byref(r) for r in rows]) \
+        == ce.CE_ERR_INVALID
+    assert b"2^32" in ce.lib().ce_last_error()
