@@ -218,6 +218,8 @@ class CmaEmitters:
         which = np.ascontiguousarray(which, np.uint32)
         if len(np.unique(which)) != len(which):
             raise ValueError("recenter: the emitters must be distinct")
+        if len(which) != len(bodies) or (len(which) and int(which.max()) >= len(self)):
+            raise ValueError("recenter: one body an emitter, emitters of this batch")
         b = take(bodies, np.arange(len(bodies)))
 
         def up(arr):

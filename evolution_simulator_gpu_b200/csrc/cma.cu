@@ -604,8 +604,12 @@ __global__ void cma_recenter_kernel(const Emitters em, const ce_population b, co
                                     uint32_t* rejected) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const uint32_t e = which[i];
+        if (e >= em.t.count) {  // no such emitter
+            if (rejected) rejected[i] = 1u;
+            continue;
+        }
         const ce_genome tg = em.t.genomes[e], bg = b.genomes[i];
-        const bool fits = e < em.t.count && bg.node_count == tg.node_count && bg.bone_count == tg.bone_count &&
+        const bool fits = bg.node_count == tg.node_count && bg.bone_count == tg.bone_count &&
                           bg.muscle_count == tg.muscle_count;
         if (rejected) rejected[i] = fits ? 0u : 1u;
         if (!fits) continue;

@@ -434,7 +434,8 @@ ce_status ce_cma_tell(const ce_cma* cma, const ce_population* samples, const flo
 /* CmaEmitter::recentered (src/qd.rs:2166-2177) for emitters which[0..n)
  * (device array, distinct emitters): emitter which[i] restarts from body i of `bodies`, which
  * must have its template's node, bone and muscle counts (else it is left as
- * it was and rejected[i], a device array or NULL, is set to 1). The body's
+ * it was and rejected[i], a device array or NULL, is set to 1; an index
+ * past the last emitter is rejected too). The body's
  * genes overwrite the template's (the templates' memory must be writable),
  * the mean moves to the body's coordinates, and the covariance, paths and
  * step size are kept when the body's plan (bone and muscle connections) is

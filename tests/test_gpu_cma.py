@@ -325,3 +325,30 @@ def test_saved_emitters_resume_where_they_stopped(engine, tmp_path):
     b = back.ask(E * 12, seed=3, generation=2, friction=(0.0, 1.0))
     for f in ("nodes", "bones", "muscles", "genomes", "strength"):
         assert (getattr(a, f).view(np.uint8) == getattr(b, f).view(np.uint8)).all()
+
+
+def test_recenter_rejects_an_emitter_past_the_last(engine):
+    import ctypes as C
+
+    import torch
+    from evolution_simulator_gpu_b200 import api
+    pop = ce.generate(SPEC, 2)
+    opt = cma.CmaEmitters(pop)
+    before = [opt.state(e) for e in range(2)]
+    b = refine.take(pop, np.array([0]))
+
+    def up(arr):
+        return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1).copy()).to(opt.device)
+
+    dn, db, dm, dg = up(b.nodes), up(b.bones), up(b.muscles), up(b.genomes)
+    which = torch.tensor([7], dtype=torch.int32, device=opt.device)
+    rej = torch.zeros(1, dtype=torch.int32, device=opt.device)
+    pc = api.PopulationC(dn.data_ptr(), db.data_ptr(), dm.data_ptr(), dg.data_ptr(), 1, None)
+    assert api.lib().ce_cma_recenter(C.byref(opt._c), C.byref(pc), which.data_ptr(), 1, rej.data_ptr(),
+                                     opt._stream.cuda_stream) == ce.CE_OK
+    assert int(rej.cpu()[0]) == 1
+    for e in range(2):
+        for x, y in zip(opt.state(e), before[e]):
+            assert (np.asarray(x) == np.asarray(y)).all()
+    with pytest.raises(ValueError):
+        opt.recenter([5], b)
